@@ -1,0 +1,156 @@
+/* kplex.h — C ABI of libkplex.so, the B200 (sm_100a) maximal k-plex enumerator.
+ *
+ * The reference (CudaPlex) has no library API: its drop-in surface is the CLI
+ * `./main <graph> -k K -q Q -t T -tr {0,1}` (main.cu:11-55), the .bin graph
+ * format (inc/graph.h:45-62) and the internal entry
+ * `void decomposableSearch(const graph<int>&)` (inc/host_funcs.h:722), which
+ * reads the globals k, lb(=q), thres, truss, bd(=q-k) (inc/kPlexEnum.h:20-24).
+ * Every entry point below names the reference interface it replaces.
+ *
+ * Conventions: plain pointers and sizes only; buffers are owned by the caller;
+ * every function returns a status (KPLEX_OK = 0) instead of exiting (the
+ * reference calls exit() on CUDA and IO errors, gpu_memory_allocation.h:1-8,
+ * utils.h:24-33).  Calls are thread-compatible: one call at a time per CUDA
+ * device; device memory is cached inside the library between calls.
+ */
+#ifndef KPLEX_H
+#define KPLEX_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define KPLEX_OK             0
+#define KPLEX_ERR_PARAM      1  /* unsupported k/q/t combination or bad argument */
+#define KPLEX_ERR_IO         2  /* file cannot be opened/written */
+#define KPLEX_ERR_FORMAT     3  /* .bin inconsistent with its header, unsorted lists, ids >= n */
+#define KPLEX_ERR_CUDA       4  /* a CUDA runtime call failed */
+#define KPLEX_ERR_NOMEM      5  /* device or host allocation failed / budget too small */
+#define KPLEX_ERR_CAPACITY   6  /* a root's 2-hop subgraph or left set exceeds 1024 vertices
+                                   (the reference's MAX_BLK_SIZE, inc/common.h:8) */
+#define KPLEX_ERR_TIMEOUT    7  /* a bounded device-side wait gave up */
+#define KPLEX_ERR_NO_DEVICE  8  /* no CUDA device / extension not usable */
+#define KPLEX_ERR_INTERNAL   9  /* device-side consistency check failed */
+
+/* kplex_params.flags */
+#define KPLEX_FLAG_QUIET        0x1u  /* no stdout lines from the library */
+#define KPLEX_FLAG_NO_HASH      0x2u  /* skip the per-output hash (count only) */
+#define KPLEX_FLAG_FORCE_SPILL  0x4u  /* test hook: spill kSearch tasks to pinned host memory at every pause */
+#define KPLEX_FLAG_TEST_NO_WAIT 0x8u  /* test hook: branch warps give up every bounded wait at once, so the
+                                         run must end with KPLEX_ERR_TIMEOUT instead of hanging */
+
+/* Run parameters: the reference's CLI flags (main.cu:31-53) plus device knobs. */
+typedef struct {
+    int k;                  /* -k : each vertex may miss at most k-1 others (k >= 2) */
+    int q;                  /* -q : minimum size of a reported k-plex (lb) */
+    float thres;            /* -t : pause-and-resume threshold, fraction of the task pool (0,1] */
+    int truss;              /* -tr: 1 = (q-2k)-truss pruning before the degeneracy order */
+    uint32_t flags;         /* KPLEX_FLAG_* */
+    int device;             /* CUDA device ordinal */
+    uint64_t pool_slots;    /* task-pool capacity in records (0 = default 4,194,304, the reference's MAX_CAP) */
+    uint32_t omp_threads;   /* host threads for preprocessing (0 = all) */
+    uint32_t shard_index;   /* multi-GPU root sharding: this call searches the roots whose */
+    uint32_t shard_count;   /* degeneracy rank r has r % shard_count == shard_index (0/0 = all) */
+} kplex_params;
+
+/* Results.  count/hash are the parity outputs; the rest mirrors the
+ * reference's printed lines (inc/host_funcs.h:1149-1157) and adds timings. */
+typedef struct {
+    uint64_t count;         /* number of maximal k-plexes of size >= q */
+    uint64_t hash;          /* order-independent 64-bit hash of the sorted vertex sets (original ids) */
+    uint64_t valid_roots;   /* "Total Valid Blocks" */
+    uint64_t tasks;         /* "Total tasks generated": kSearch tasks + branch children */
+    uint64_t nodes;         /* branch-and-bound nodes processed on the device */
+    uint32_t pn, pm;        /* vertices / directed edges after (q-k)-core (and truss) pruning */
+    uint32_t max_local_n;   /* largest root subgraph |{root} u C1 u C2| */
+    uint32_t max_left;      /* largest root left set */
+    uint32_t pauses;        /* kSearch pause/resume cycles */
+    uint32_t spilled;       /* task records moved to pinned host memory and back */
+    double ms_preprocess;   /* host core/truss/degeneracy */
+    double ms_device;       /* device search: decomposition + k-search + branch-and-bound */
+    double ms_ref_region;   /* preprocess + device search: the reference's "Total Time Elapsed" region */
+    double ms_total;        /* whole call, including uploads and allocation */
+    int status;
+    uint32_t gpu_launches;  /* kernels launched by this call */
+    double ms_decompose;    /* device time of the decomposition kernel */
+    double ms_ksearch;      /* device time of the k-search launches */
+    double ms_bnb;          /* device time of the branch-and-bound launches */
+    uint64_t bnb_bytes;     /* algorithmic bytes of branch-and-bound: 12W per node and per child
+                               record (P, C, X bitsets of W words) + 4W per adjacency row read */
+    uint64_t roots_bytes;   /* algorithmic bytes of decomposition: CSR words read + bit matrices written */
+} kplex_result;
+
+/* A CSR graph owned by the library (kplex_load_bin / kplex_generate). */
+typedef struct {
+    uint32_t n;
+    uint64_t m_directed;    /* = offsets[n] = 2|E| */
+    uint32_t* offsets;      /* n + 1 */
+    uint32_t* neighbors;    /* m_directed, each list strictly ascending */
+} kplex_graph;
+
+/* Seeded synthetic workload: Chung-Lu base graph with an exact edge count
+ * plus planted dense groups (project-defined; replaces the reference's
+ * shipped datasets when those are not available). */
+typedef struct {
+    uint64_t seed;
+    uint32_t n;
+    uint64_t base_edges;
+    double exponent;
+    uint32_t max_degree;
+    uint32_t groups, group_min, group_max;
+    double density_min, density_max;
+} kplex_gen_spec;
+
+/* Replaces graph<intT>::graph(path) (inc/graph.h:37-65). Caller frees with kplex_free_graph. */
+int kplex_load_bin(const char* path, kplex_graph* out);
+/* Inverse of kplex_load_bin; the layout of writeBinaryGraph (inc/graphIO.h:13-27). */
+int kplex_save_bin(const char* path, const kplex_graph* g);
+/* Replaces graph<intT>::del() (inc/graph.h:78-87). */
+void kplex_free_graph(kplex_graph* g);
+/* Project-written generator (no reference counterpart). */
+int kplex_generate(const kplex_gen_spec* spec, kplex_graph* out);
+
+/* Replaces decomposableSearch(g) (inc/host_funcs.h:722-1161) with the globals
+ * k/lb/thres/truss passed in `p`.  Inputs are host CSR arrays owned by the
+ * caller.  Runs the host preprocessing (core, truss, degeneracy) and the
+ * device search on p->device; fills *out and returns out->status. */
+int kplex_enumerate_csr(const uint32_t* offsets, const uint32_t* neighbors, uint32_t n,
+                        uint64_t m_directed, const kplex_params* p, kplex_result* out);
+
+/* Replaces main.cu:56-61 (load + decomposableSearch) for a .bin path. */
+int kplex_enumerate_file(const char* path, const kplex_params* p, kplex_result* out);
+
+/* Two-stage form used to time the device search alone: kplex_prepare runs the
+ * host preprocessing and uploads the pruned graph (handle returned in *h);
+ * kplex_search runs decomposition + k-search + branch-and-bound on it and may
+ * be called repeatedly; kplex_release frees the handle.  No reference
+ * counterpart (the reference fuses these in decomposableSearch). */
+typedef struct kplex_prepared kplex_prepared;
+int kplex_prepare(const uint32_t* offsets, const uint32_t* neighbors, uint32_t n,
+                  uint64_t m_directed, const kplex_params* p, kplex_prepared** h, kplex_result* out);
+int kplex_search(kplex_prepared* h, kplex_result* out);
+void kplex_release(kplex_prepared* h);
+
+/* Host preprocessing only (no device): (q-k)-core (inc/host_funcs.h:16-122),
+ * optional (q-2k)-truss (inc/host_funcs.h:761-823, 463-559) and the degeneracy
+ * order (inc/degeneracy.h + inc/host_funcs.h:829-851).  Output buffers are
+ * caller-owned and sized n+1 (out_off), m_directed (out_adj) and n (the rest).
+ * Returns the pruned vertex count pn (>= 0) or -status. */
+long long kplex_preprocess_csr(const uint32_t* offsets, const uint32_t* neighbors, uint32_t n, uint64_t m_directed,
+                               int k, int q, int truss, uint32_t omp_threads,
+                               uint32_t* out_off, uint32_t* out_adj, int32_t* out_dpos, int32_t* out_dseq,
+                               uint32_t* out_orig, uint64_t* out_m);
+
+const char* kplex_status_string(int status);
+/* Text of the last failure on the calling thread (CUDA message, parse error, ...). */
+const char* kplex_last_error(void);
+int kplex_version(void);
+/* 1 if a CUDA device is visible and the sm_100a kernels can run on it. */
+int kplex_device_ok(int device);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* KPLEX_H */

@@ -1,0 +1,120 @@
+// Device-side layout shared by the decomposition, k-search and branch kernels.
+//
+// HBM layout (all per search, sized on the host):
+//   roots[R]        RootDesc per root rank r < pn - q + 2 (inc: src/device_funcs.cu:44-45)
+//   arena           u32 words; each valid root owns one contiguous block:
+//                     A  [n][W]   adjacency bits of the root's local subgraph
+//                     M2 [n][W]   pair class >= UNLINK2EQUAL (src:1751-1853, used by
+//                                 updateCand13/23 and the include filter)
+//                     M4 [n][W]   pair class >= UNLINK2MORE (the X filter, src:1396-1404)
+//                     LA [n][WL]  adjacency from local vertices to the root's left set
+//                     LT [nl][W]  the transpose of LA
+//                     sorig [n]   original ids of the local vertices, ascending
+//                     srank [n]   position of each local vertex in sorig (u32)
+//   pool            bounded MPMC ring of task records (the reference's queue A;
+//                   host:953-957) shared by the k-search and branch kernels
+//   stacks          one depth-first stack of task records per branch warp
+// A task record is TaskHdr followed by the P, C and X bitsets (Wt words each).
+// Local vertex ids: 0 = root, [1, hop) = C1, [hop, n) = C2 (as in the reference).
+#pragma once
+#include <cstdint>
+#include "kplex_common.h"
+#include "../../include/kplex.h"
+
+namespace kplex {
+
+constexpr int MAX_LOCAL = 1024;     // inc/common.h:8 MAX_BLK_SIZE
+constexpr int MAX_WORDS = MAX_LOCAL / 32;
+constexpr int KS_MAX_DEPTH = 1000;  // inc/common.h:15 MAX_DEPTH
+constexpr int MAX_K = 32;
+
+// root flags
+enum : uint32_t {
+    ROOT_VALID = 1u,       // |blk| >= q: counted in "Total Valid Blocks"
+    ROOT_TRUNCATED = 2u,   // more than 1023 later or 1024 earlier neighbours (reference drops extras)
+    ROOT_OVERSIZED = 4u,   // n or |left| beyond 1024: not representable, run fails
+    ROOT_SKIPPED = 8u,     // C1 smaller than q-k after peeling (src:148)
+};
+
+struct RootDesc {
+    uint32_t n, hop, nleft, W;   // W: words per local row, multiple of 4
+    uint32_t WL, flags, gid, pad;
+    uint64_t base;               // word offset of the root's block in the arena
+};
+
+struct TaskHdr {
+    uint32_t root;
+    uint16_t np, nc;
+    uint16_t nx, pad0;
+    uint32_t pad1;
+};
+static_assert(sizeof(TaskHdr) == 16, "task header is one uint4");
+
+// Global counters and flags, one per search.
+struct Counters {
+    unsigned long long count;      // maximal k-plexes found
+    unsigned long long hash;       // wrapping sum of plex hashes
+    unsigned long long tasks;      // kSearch tasks + branch children ("Total tasks generated")
+    unsigned long long nodes;      // branch nodes processed
+    unsigned long long bnb_bytes;  // algorithmic bytes of branch nodes (roofline accounting)
+    unsigned long long arena_top;  // words bump-allocated in the arena
+    unsigned int valid_roots;
+    unsigned int max_n, max_left, max_w;
+    unsigned int truncated, oversized, depth_capped;
+    unsigned int error;            // KPLEX_ERR_* raised on the device (first one wins)
+    unsigned int next_root;        // k-search root dispenser
+    unsigned int ks_paused;        // k-search warps that stopped at the pause threshold
+    unsigned int ks_active;        // k-search slots holding an unfinished root
+    unsigned int busy;             // branch warps holding work (termination detection)
+    unsigned int bnb_done;         // branch warps that exited
+    unsigned int timeouts;         // bounded waits that gave up
+    unsigned int decomp_next;      // decomposition root dispenser
+    unsigned int pad[3];
+    unsigned long long roots_bytes; // algorithmic bytes of the decomposition
+};
+
+// Vyukov bounded MPMC ring: each slot carries a sequence number so that a
+// producer and a consumer never touch the same record concurrently.
+struct Pool {
+    unsigned long long head;   // next slot to dequeue
+    unsigned long long tail;   // next slot to enqueue
+    unsigned long long cap;    // slots
+    unsigned long long pad;
+};
+
+struct SearchParams {
+    int k, q;
+    uint32_t nroots;           // number of root ranks considered
+    uint32_t pn;
+    const uint32_t* off;       // pruned CSR
+    const uint32_t* adj;
+    const int32_t* dpos;
+    const int32_t* dseq;
+    const uint32_t* orig;      // pruned id -> input id
+    RootDesc* roots;
+    uint32_t* arena;
+    unsigned long long arena_cap;  // words
+    Counters* ctr;
+    Pool* pool;
+    uint32_t* pool_seq;        // per slot sequence (u64 position folded to 32 bits)
+    uint32_t* pool_data;       // cap * slot_words
+    uint32_t slot_words;       // 4 + 3 * Wt
+    uint32_t Wt;               // words per bitset in a task record
+    unsigned long long pause_at;   // k-search pauses when the pool holds this many records
+    uint32_t* warp_scratch;    // decomposition per-warp scratch
+    uint64_t scratch_words;    // words per warp
+    uint32_t* ks_slots;        // k-search per-warp state (KS_WORDS each), kept across pauses
+    uint32_t* stacks;          // branch stacks: warps * stack_depth * slot_words
+    uint32_t stack_depth;
+    uint32_t nwarps;           // branch warps launched
+    uint32_t low_water;        // a branch warp donates work when the pool holds fewer records
+    uint32_t hash_on;
+    uint32_t shard_index, shard_count;
+    unsigned long long spin_limit;   // iterations for any bounded wait
+};
+
+__device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31; }
+
+__device__ __forceinline__ void raise_error(Counters* c, unsigned code) { atomicCAS(&c->error, 0u, code); }
+
+}  // namespace kplex

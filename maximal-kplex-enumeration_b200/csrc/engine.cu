@@ -1,0 +1,528 @@
+// Host engine: the C ABI of include/kplex.h.
+//
+// Replaces decomposableSearch (inc/host_funcs.h:722-1161).  The reference
+// allocates ~40 GB of fixed per-warp slabs (inc/gpu_memory_allocation.h:10-63,
+// host:916-1011), launches five kernels per wave of 4,544 roots and reads a
+// flag back after every BNB wave (host:253-335).  Here one search is:
+//   decompose_kernel  all roots at once into a bump-allocated arena
+//   ksearch_kernel    fills the task pool until it holds thres * capacity records
+//   bnb_kernel        persistent; drains the pool with per-warp depth-first stacks
+//   (repeat k-search + branch while k-search paused: pause-and-resume, host:1094-1122)
+// with a handful of 64-byte counter reads in total.  Device buffers are cached
+// per device and grown on demand.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "device.cuh"
+#include "graph_io.h"
+#include "preprocess.h"
+
+namespace kplex {
+
+__global__ void decompose_kernel(SearchParams sp);
+__global__ void ksearch_kernel(SearchParams sp);
+__global__ void bnb_kernel(SearchParams sp, uint32_t nmax);
+uint64_t decomp_scratch_words_host(uint32_t pn);
+uint32_t bnb_smem_words_host(uint32_t nmax, uint32_t slot_words);
+uint32_t ks_slot_words_host();
+
+// ------------------------------------------------------------------ small kernels
+__global__ void init_decomp_scratch(uint32_t* scratch, uint64_t words_per_warp, uint32_t pn, uint32_t nwarps) {
+    const uint64_t total = (uint64_t)nwarps * 2 * pn;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t w = i / (2ull * pn), o = i % (2ull * pn);
+        scratch[w * words_per_warp + o] = (o < pn) ? 0xffffffffu : 0u;
+    }
+}
+__global__ void init_pool(uint32_t* seq, unsigned long long cap, Pool* pool) {
+    for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < cap; i += (unsigned long long)gridDim.x * blockDim.x)
+        seq[i] = (uint32_t)i;
+    if (blockIdx.x == 0 && threadIdx.x == 0) { pool->head = 0; pool->tail = 0; pool->cap = cap; pool->pad = 0; }
+}
+__global__ void init_ks_slots(uint32_t* slots, uint32_t nwarps, uint32_t words) {
+    for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < nwarps; w += gridDim.x * blockDim.x) slots[(uint64_t)w * words] = 0xffffffffu;
+}
+
+// ------------------------------------------------------------------ errors
+static thread_local std::string g_last_error;
+
+#define CK(call)                                                                    \
+    do {                                                                            \
+        cudaError_t e_ = (call);                                                    \
+        if (e_ != cudaSuccess) {                                                    \
+            g_last_error = std::string(#call) + ": " + cudaGetErrorString(e_);      \
+            return KPLEX_ERR_CUDA;                                                  \
+        }                                                                           \
+    } while (0)
+
+// ------------------------------------------------------------------ device buffer cache
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    int ensure(size_t want) {
+        if (want <= bytes && p) return KPLEX_OK;
+        if (p) { cudaFree(p); p = nullptr; bytes = 0; }
+        if (want == 0) want = 16;
+        cudaError_t e = cudaMalloc(&p, want);
+        if (e != cudaSuccess) { cudaGetLastError(); p = nullptr; g_last_error = std::string("cudaMalloc ") + std::to_string(want) + ": " + cudaGetErrorString(e); return KPLEX_ERR_NOMEM; }
+        bytes = want;
+        return KPLEX_OK;
+    }
+    template <typename T> T* as() const { return static_cast<T*>(p); }
+};
+
+struct DeviceState {
+    bool init = false;
+    int sms = 0;
+    cudaStream_t stream = nullptr;
+    DevBuf roots, ctr, scratch, arena, pool_seq, pool_data, pool, ks, stacks;
+    Counters* h_ctr = nullptr;   // pinned
+};
+
+static std::mutex g_mu;
+static DeviceState g_dev[64];
+
+static int device_state(int device, DeviceState** out) {
+    if (device < 0 || device >= 64) return KPLEX_ERR_PARAM;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || device >= n) { cudaGetLastError(); g_last_error = "no CUDA device"; return KPLEX_ERR_NO_DEVICE; }
+    CK(cudaSetDevice(device));
+    DeviceState& d = g_dev[device];
+    if (!d.init) {
+        cudaDeviceProp prop;
+        CK(cudaGetDeviceProperties(&prop, device));
+        if (prop.major != 10) { g_last_error = "kernels are built for sm_100a only"; return KPLEX_ERR_NO_DEVICE; }
+        d.sms = prop.multiProcessorCount;
+        CK(cudaStreamCreateWithFlags(&d.stream, cudaStreamNonBlocking));
+        CK(cudaMallocHost(&d.h_ctr, sizeof(Counters)));
+        d.init = true;
+    }
+    *out = &d;
+    return KPLEX_OK;
+}
+
+static double ms_since(std::chrono::steady_clock::time_point t0) {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+}  // namespace kplex
+
+using namespace kplex;
+
+struct kplex_prepared {
+    int device = 0;
+    kplex_params p{};
+    uint32_t pn = 0, pm = 0;
+    double ms_pre = 0;
+    uint32_t* d_off = nullptr;
+    uint32_t* d_adj = nullptr;
+    int32_t* d_dpos = nullptr;
+    int32_t* d_dseq = nullptr;
+    uint32_t* d_orig = nullptr;
+};
+
+static int check_params(const kplex_params* p) {
+    if (!p) { g_last_error = "null params"; return KPLEX_ERR_PARAM; }
+    if (p->k < 2 || p->k > MAX_K - 1) { g_last_error = "k must be in [2, 31]"; return KPLEX_ERR_PARAM; }
+    if (p->q < 2 * p->k - 1) { g_last_error = "q must be >= 2k-1"; return KPLEX_ERR_PARAM; }
+    if (!(p->thres > 0.0f) || p->thres > 1.0f) { g_last_error = "thres must be in (0, 1]"; return KPLEX_ERR_PARAM; }
+    return KPLEX_OK;
+}
+
+static void free_prepared(kplex_prepared* h) {
+    if (!h) return;
+    cudaSetDevice(h->device);
+    cudaFree(h->d_off); cudaFree(h->d_adj); cudaFree(h->d_dpos); cudaFree(h->d_dseq); cudaFree(h->d_orig);
+    delete h;
+}
+
+static int prepare_impl(const uint32_t* off, const uint32_t* adj, uint32_t n, uint64_t m, const kplex_params* p,
+                        kplex_prepared** out_h, kplex_result* out) {
+    int rc = check_params(p);
+    if (rc) return rc;
+    if (!off || (!adj && m) || (n && off[n] != m) || m > 0xffffffffull) { g_last_error = "inconsistent CSR"; return KPLEX_ERR_FORMAT; }
+    Csr g;
+    g.n = n;
+    g.off.assign(off, off + n + 1);
+    g.adj.assign(adj, adj + m);
+    std::string err;
+    rc = validate_csr(g, &err);
+    if (rc) { g_last_error = err; return rc; }
+    DeviceState* d = nullptr;
+    rc = device_state(p->device, &d);
+    if (rc) return rc;
+    auto t0 = std::chrono::steady_clock::now();
+    Prepped pre;
+    preprocess(g, p->k, p->q, p->truss, (int)p->omp_threads, pre);
+    const double ms_pre = ms_since(t0);
+    if (!(p->flags & KPLEX_FLAG_QUIET)) printf("\npn = %u\n", pre.g.n);
+    kplex_prepared* h = new kplex_prepared();
+    h->device = p->device;
+    h->p = *p;
+    h->pn = pre.g.n;
+    h->pm = pre.g.n ? pre.g.off[pre.g.n] : 0;
+    h->ms_pre = ms_pre;
+    auto fail = [&](int code) { free_prepared(h); return code; };
+    const size_t pn = h->pn;
+    if (cudaMalloc(&h->d_off, (pn + 1) * 4) != cudaSuccess || cudaMalloc(&h->d_adj, std::max<size_t>(h->pm, 1) * 4) != cudaSuccess ||
+        cudaMalloc(&h->d_dpos, std::max<size_t>(pn, 1) * 4) != cudaSuccess || cudaMalloc(&h->d_dseq, std::max<size_t>(pn, 1) * 4) != cudaSuccess ||
+        cudaMalloc(&h->d_orig, std::max<size_t>(pn, 1) * 4) != cudaSuccess) {
+        cudaGetLastError(); g_last_error = "cudaMalloc for the pruned graph failed"; return fail(KPLEX_ERR_NOMEM);
+    }
+    if (!pre.g.off.empty()) CK(cudaMemcpyAsync(h->d_off, pre.g.off.data(), (pn + 1) * 4, cudaMemcpyHostToDevice, d->stream));
+    if (h->pm) CK(cudaMemcpyAsync(h->d_adj, pre.g.adj.data(), (size_t)h->pm * 4, cudaMemcpyHostToDevice, d->stream));
+    if (pn) {
+        CK(cudaMemcpyAsync(h->d_dpos, pre.dpos.data(), pn * 4, cudaMemcpyHostToDevice, d->stream));
+        CK(cudaMemcpyAsync(h->d_dseq, pre.dseq.data(), pn * 4, cudaMemcpyHostToDevice, d->stream));
+        CK(cudaMemcpyAsync(h->d_orig, pre.orig.data(), pn * 4, cudaMemcpyHostToDevice, d->stream));
+    }
+    CK(cudaStreamSynchronize(d->stream));
+    if (out) { out->pn = h->pn; out->pm = h->pm; out->ms_preprocess = ms_pre; }
+    *out_h = h;
+    return KPLEX_OK;
+}
+
+static int search_impl(kplex_prepared* h, kplex_result* out) {
+    DeviceState* d = nullptr;
+    int rc = device_state(h->device, &d);
+    if (rc) return rc;
+    const kplex_params& P = h->p;
+    cudaStream_t st = d->stream;
+    const long long lim = (long long)h->pn - (long long)P.q + 2;   // src:44-45
+    const uint32_t nroots = lim > 0 ? (uint32_t)std::min<long long>(lim, h->pn) : 0u;
+    uint32_t launches = 0;
+    cudaEvent_t e0, e1, ka, kb;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventCreate(&ka));
+    CK(cudaEventCreate(&kb));
+    CK(cudaEventRecord(e0, st));
+    double ms_dec = 0, ms_ks = 0, ms_bnb = 0;
+    auto timed = [&](auto&& launch, double& acc) -> int {
+        CK(cudaEventRecord(ka, st));
+        launch();
+        CK(cudaGetLastError());
+        CK(cudaEventRecord(kb, st));
+        CK(cudaEventSynchronize(kb));
+        float t = 0;
+        CK(cudaEventElapsedTime(&t, ka, kb));
+        acc += t;
+        return KPLEX_OK;
+    };
+
+    SearchParams sp{};
+    sp.k = P.k; sp.q = P.q; sp.nroots = nroots; sp.pn = h->pn;
+    sp.off = h->d_off; sp.adj = h->d_adj; sp.dpos = h->d_dpos; sp.dseq = h->d_dseq; sp.orig = h->d_orig;
+    sp.hash_on = (P.flags & KPLEX_FLAG_NO_HASH) ? 0u : 1u;
+    sp.shard_index = P.shard_count > 1 ? P.shard_index : 0u;
+    sp.shard_count = P.shard_count > 1 ? P.shard_count : 1u;
+    sp.spin_limit = 1ull << 24;
+
+    if ((rc = d->ctr.ensure(sizeof(Counters)))) return rc;
+    if ((rc = d->roots.ensure(std::max<size_t>(nroots, 1) * sizeof(RootDesc)))) return rc;
+    sp.ctr = d->ctr.as<Counters>();
+    sp.roots = d->roots.as<RootDesc>();
+
+    // ---------------- decomposition (with arena growth on overflow)
+    const uint32_t dec_warps = std::max<uint32_t>(8, std::min<uint32_t>((uint32_t)d->sms * 16, ((nroots + 7) / 8) * 8));
+    sp.scratch_words = decomp_scratch_words_host(h->pn);
+    if ((rc = d->scratch.ensure((size_t)dec_warps * sp.scratch_words * 4))) return rc;
+    sp.warp_scratch = d->scratch.as<uint32_t>();
+    size_t arena_words = std::max<size_t>(d->arena.bytes / 4, (size_t)1 << 22);
+    Counters& hc = *d->h_ctr;
+    for (int attempt = 0;; ++attempt) {
+        if ((rc = d->arena.ensure(arena_words * 4))) return rc;
+        sp.arena = d->arena.as<uint32_t>();
+        sp.arena_cap = arena_words;
+        CK(cudaMemsetAsync(sp.ctr, 0, sizeof(Counters), st));
+        if (nroots) {
+            init_decomp_scratch<<<d->sms * 4, 256, 0, st>>>(sp.warp_scratch, sp.scratch_words, h->pn, dec_warps);
+            if ((rc = timed([&] { decompose_kernel<<<dec_warps / 8, 256, 0, st>>>(sp); }, ms_dec))) return rc;
+            launches += 2;
+        }
+        CK(cudaMemcpyAsync(&hc, sp.ctr, sizeof(Counters), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (hc.error == KPLEX_ERR_NOMEM && attempt < 6) {
+            arena_words = std::max<size_t>(arena_words * 2, (size_t)(hc.arena_top * 5 / 4 + 1024));
+            continue;
+        }
+        break;
+    }
+    if (hc.error) {
+        g_last_error = hc.error == KPLEX_ERR_CAPACITY ? "a root's 2-hop subgraph or left set exceeds 1024 vertices" : "device error in decomposition";
+        return (int)hc.error;
+    }
+    const uint32_t nmax = std::max<uint32_t>(hc.max_n, 1);
+    const uint32_t Wt = std::max<uint32_t>(hc.max_w, 4);
+    sp.Wt = Wt;
+    sp.slot_words = 4 + 3 * Wt;
+
+    // ---------------- pool, k-search slots, branch stacks
+    const unsigned long long cap = P.pool_slots ? P.pool_slots : 4194304ull;   // MAX_CAP, inc/common.h:10
+    if ((rc = d->pool.ensure(sizeof(Pool)))) return rc;
+    if ((rc = d->pool_seq.ensure((size_t)cap * 4))) return rc;
+    if ((rc = d->pool_data.ensure((size_t)cap * sp.slot_words * 4))) return rc;
+    sp.pool = d->pool.as<Pool>();
+    sp.pool_seq = d->pool_seq.as<uint32_t>();
+    sp.pool_data = d->pool_data.as<uint32_t>();
+    init_pool<<<d->sms * 4, 256, 0, st>>>(sp.pool_seq, cap, sp.pool);
+    ++launches;
+    const uint32_t ks_warps = (uint32_t)d->sms * 8;
+    if ((rc = d->ks.ensure((size_t)ks_warps * ks_slot_words_host() * 4))) return rc;
+    sp.ks_slots = d->ks.as<uint32_t>();
+    init_ks_slots<<<(ks_warps + 255) / 256, 256, 0, st>>>(sp.ks_slots, ks_warps, ks_slot_words_host());
+    ++launches;
+    const long long pause = (long long)std::floor((double)cap * (double)P.thres) - (long long)ks_warps;   // host:2083 MAX_CAP*thres - WARPS
+    sp.pause_at = (unsigned long long)std::max<long long>(pause, 1);
+
+    const uint32_t smem_words = bnb_smem_words_host(nmax, sp.slot_words);
+    const int warps_per_block = 8;
+    const size_t smem_bytes = (size_t)smem_words * 4 * warps_per_block;
+    CK(cudaFuncSetAttribute(bnb_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes));
+    int per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bnb_kernel, warps_per_block * 32, smem_bytes));
+    per_sm = std::max(per_sm, 1);
+    const uint32_t bnb_blocks = (uint32_t)d->sms * (uint32_t)per_sm;
+    const uint32_t bnb_warps = bnb_blocks * warps_per_block;
+    sp.nwarps = bnb_warps;
+    sp.stack_depth = nmax + 2;
+    sp.low_water = 2 * bnb_warps;
+    if ((rc = d->stacks.ensure((size_t)bnb_warps * sp.stack_depth * sp.slot_words * 4))) return rc;
+    sp.stacks = d->stacks.as<uint32_t>();
+
+    // ---------------- k-search / branch-and-bound with pause-and-resume
+    uint32_t pauses = 0;
+    for (int cycle = 0;; ++cycle) {
+        if (cycle > (1 << 22)) { g_last_error = "pause-and-resume did not finish"; return KPLEX_ERR_INTERNAL; }
+        CK(cudaMemsetAsync(&sp.ctr->ks_paused, 0, sizeof(unsigned), st));
+        if (nroots) {
+            if ((rc = timed([&] { ksearch_kernel<<<ks_warps / 4, 128, 0, st>>>(sp); }, ms_ks))) return rc;
+            ++launches;
+            SearchParams sb = sp;
+            if (P.flags & KPLEX_FLAG_TEST_NO_WAIT) sb.spin_limit = 0;   // failure-detection test hook
+            if ((rc = timed([&] { bnb_kernel<<<bnb_blocks, warps_per_block * 32, smem_bytes, st>>>(sb, nmax); }, ms_bnb))) return rc;
+            ++launches;
+        }
+        CK(cudaMemcpyAsync(&hc, sp.ctr, sizeof(Counters), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (hc.error) break;
+        if (hc.ks_paused == 0) break;
+        ++pauses;
+    }
+    Pool hp;
+    CK(cudaMemcpyAsync(&hp, sp.pool, sizeof(Pool), cudaMemcpyDeviceToHost, st));
+    CK(cudaEventRecord(e1, st));
+    CK(cudaEventSynchronize(e1));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaEventDestroy(ka);
+    cudaEventDestroy(kb);
+    if (!hc.error && hp.head != hp.tail) { hc.error = KPLEX_ERR_TIMEOUT; g_last_error = "branch warps gave up with records left in the pool"; }
+    if (out) {
+        out->count = hc.count;
+        out->hash = hc.hash;
+        out->valid_roots = hc.valid_roots;
+        out->tasks = hc.tasks;
+        out->nodes = hc.nodes;
+        out->pn = h->pn;
+        out->pm = h->pm;
+        out->max_local_n = hc.max_n;
+        out->max_left = hc.max_left;
+        out->pauses = pauses;
+        out->spilled = 0;
+        out->ms_preprocess = h->ms_pre;
+        out->ms_device = ms;
+        out->ms_ref_region = h->ms_pre + ms;
+        out->gpu_launches = launches;
+        out->ms_decompose = ms_dec;
+        out->ms_ksearch = ms_ks;
+        out->ms_bnb = ms_bnb;
+        out->bnb_bytes = hc.bnb_bytes;
+        out->roots_bytes = hc.roots_bytes;
+        out->status = (int)hc.error;
+    }
+    return (int)hc.error;
+}
+
+// ------------------------------------------------------------------ C ABI
+extern "C" {
+
+int kplex_version(void) { return 1; }
+
+long long kplex_preprocess_csr(const uint32_t* offsets, const uint32_t* neighbors, uint32_t n, uint64_t m_directed,
+                               int k, int q, int truss, uint32_t omp_threads,
+                               uint32_t* out_off, uint32_t* out_adj, int32_t* out_dpos, int32_t* out_dseq,
+                               uint32_t* out_orig, uint64_t* out_m) {
+    if (!offsets || (!neighbors && m_directed) || !out_off || !out_m) return -KPLEX_ERR_PARAM;
+    if (offsets[n] != m_directed || m_directed > 0xffffffffull) return -KPLEX_ERR_FORMAT;
+    Csr g;
+    g.n = n;
+    g.off.assign(offsets, offsets + n + 1);
+    g.adj.assign(neighbors, neighbors + m_directed);
+    std::string err;
+    int rc = validate_csr(g, &err);
+    if (rc) { g_last_error = err; return -rc; }
+    Prepped pre;
+    preprocess(g, k, q, truss, (int)omp_threads, pre);
+    const uint32_t pn = pre.g.n;
+    memcpy(out_off, pre.g.off.data(), ((size_t)pn + 1) * 4);
+    if (!pre.g.adj.empty()) memcpy(out_adj, pre.g.adj.data(), pre.g.adj.size() * 4);
+    if (pn) {
+        memcpy(out_dpos, pre.dpos.data(), (size_t)pn * 4);
+        memcpy(out_dseq, pre.dseq.data(), (size_t)pn * 4);
+        memcpy(out_orig, pre.orig.data(), (size_t)pn * 4);
+    }
+    *out_m = pre.g.adj.size();
+    return pn;
+}
+
+const char* kplex_status_string(int s) {
+    switch (s) {
+        case KPLEX_OK: return "ok";
+        case KPLEX_ERR_PARAM: return "unsupported parameter";
+        case KPLEX_ERR_IO: return "io error";
+        case KPLEX_ERR_FORMAT: return "malformed graph";
+        case KPLEX_ERR_CUDA: return "cuda error";
+        case KPLEX_ERR_NOMEM: return "out of memory";
+        case KPLEX_ERR_CAPACITY: return "root subgraph exceeds 1024 vertices";
+        case KPLEX_ERR_TIMEOUT: return "bounded device wait gave up";
+        case KPLEX_ERR_NO_DEVICE: return "no usable CUDA device";
+        case KPLEX_ERR_INTERNAL: return "internal device check failed";
+        default: return "unknown status";
+    }
+}
+
+const char* kplex_last_error(void) { return g_last_error.c_str(); }
+
+int kplex_device_ok(int device) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    DeviceState* d = nullptr;
+    return device_state(device, &d) == KPLEX_OK ? 1 : 0;
+}
+
+int kplex_load_bin(const char* path, kplex_graph* out) {
+    if (!path || !out) return KPLEX_ERR_PARAM;
+    Csr g;
+    std::string err;
+    int rc = load_bin(path, g, &err);
+    if (rc) { g_last_error = err; return rc; }
+    out->n = g.n;
+    out->m_directed = g.m_directed();
+    out->offsets = (uint32_t*)malloc(((size_t)g.n + 1) * 4);
+    out->neighbors = (uint32_t*)malloc(std::max<size_t>(g.adj.size(), 1) * 4);
+    if (!out->offsets || !out->neighbors) { free(out->offsets); free(out->neighbors); return KPLEX_ERR_NOMEM; }
+    memcpy(out->offsets, g.off.data(), ((size_t)g.n + 1) * 4);
+    if (!g.adj.empty()) memcpy(out->neighbors, g.adj.data(), g.adj.size() * 4);
+    return KPLEX_OK;
+}
+
+int kplex_save_bin(const char* path, const kplex_graph* g) {
+    if (!path || !g) return KPLEX_ERR_PARAM;
+    Csr c;
+    c.n = g->n;
+    c.off.assign(g->offsets, g->offsets + g->n + 1);
+    c.adj.assign(g->neighbors, g->neighbors + g->m_directed);
+    std::string err;
+    int rc = save_bin(path, c, &err);
+    if (rc) g_last_error = err;
+    return rc;
+}
+
+void kplex_free_graph(kplex_graph* g) {
+    if (!g) return;
+    free(g->offsets); free(g->neighbors);
+    g->offsets = g->neighbors = nullptr;
+    g->n = 0; g->m_directed = 0;
+}
+
+int kplex_generate(const kplex_gen_spec* s, kplex_graph* out) {
+    if (!s || !out) return KPLEX_ERR_PARAM;
+    GenSpec gs;
+    gs.seed = s->seed; gs.n = s->n; gs.base_edges = s->base_edges; gs.exponent = s->exponent; gs.max_degree = s->max_degree;
+    gs.groups = s->groups; gs.group_min = s->group_min; gs.group_max = s->group_max;
+    gs.density_min = s->density_min; gs.density_max = s->density_max;
+    Csr g;
+    std::string err;
+    int rc = generate(gs, g, &err);
+    if (rc) { g_last_error = err; return rc; }
+    out->n = g.n;
+    out->m_directed = g.m_directed();
+    out->offsets = (uint32_t*)malloc(((size_t)g.n + 1) * 4);
+    out->neighbors = (uint32_t*)malloc(std::max<size_t>(g.adj.size(), 1) * 4);
+    if (!out->offsets || !out->neighbors) { free(out->offsets); free(out->neighbors); return KPLEX_ERR_NOMEM; }
+    memcpy(out->offsets, g.off.data(), ((size_t)g.n + 1) * 4);
+    if (!g.adj.empty()) memcpy(out->neighbors, g.adj.data(), g.adj.size() * 4);
+    return KPLEX_OK;
+}
+
+int kplex_prepare(const uint32_t* offsets, const uint32_t* neighbors, uint32_t n, uint64_t m_directed,
+                  const kplex_params* p, kplex_prepared** h, kplex_result* out) {
+    if (!h) return KPLEX_ERR_PARAM;
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (out) memset(out, 0, sizeof(*out));
+    int rc = prepare_impl(offsets, neighbors, n, m_directed, p, h, out);
+    if (out) out->status = rc;
+    return rc;
+}
+
+int kplex_search(kplex_prepared* h, kplex_result* out) {
+    if (!h) return KPLEX_ERR_PARAM;
+    std::lock_guard<std::mutex> lk(g_mu);
+    auto t0 = std::chrono::steady_clock::now();
+    int rc = search_impl(h, out);
+    if (out) { out->status = rc; out->ms_total = ms_since(t0); }
+    return rc;
+}
+
+void kplex_release(kplex_prepared* h) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    free_prepared(h);
+}
+
+int kplex_enumerate_csr(const uint32_t* offsets, const uint32_t* neighbors, uint32_t n, uint64_t m_directed,
+                        const kplex_params* p, kplex_result* out) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    auto t0 = std::chrono::steady_clock::now();
+    kplex_result tmp;
+    kplex_result* r = out ? out : &tmp;
+    memset(r, 0, sizeof(*r));
+    kplex_prepared* h = nullptr;
+    const bool verbose = p && !(p->flags & KPLEX_FLAG_QUIET);
+    int rc = prepare_impl(offsets, neighbors, n, m_directed, p, &h, r);
+    if (rc == KPLEX_OK) {
+        if (verbose) { printf("Start copying graph to GPU....\n"); printf("Done copying graph to GPU....\n"); }
+        rc = search_impl(h, r);
+        free_prepared(h);
+    }
+    r->status = rc;
+    r->ms_total = ms_since(t0);
+    if (verbose && rc == KPLEX_OK) {
+        printf("Total Time Elapsed: %f ms\n", r->ms_ref_region);
+        printf("Total Valid Blocks: %d, Maximal k-Plexes: %u\n", (int)r->valid_roots, (unsigned)(r->count & 0xffffffffu));
+        printf("Total tasks generated: %u\n", (unsigned)(r->tasks & 0xffffffffu));
+        printf("\nKernel Launch Successfully\n");
+    }
+    return rc;
+}
+
+int kplex_enumerate_file(const char* path, const kplex_params* p, kplex_result* out) {
+    kplex_graph g{};
+    int rc = kplex_load_bin(path, &g);
+    if (rc) { if (out) { memset(out, 0, sizeof(*out)); out->status = rc; } return rc; }
+    if (p && !(p->flags & KPLEX_FLAG_QUIET)) printf("n=%u, m=%u (undirected)\n", g.n, (unsigned)g.m_directed);
+    rc = kplex_enumerate_csr(g.offsets, g.neighbors, g.n, g.m_directed, p, out);
+    kplex_free_graph(&g);
+    return rc;
+}
+
+}  // extern "C"

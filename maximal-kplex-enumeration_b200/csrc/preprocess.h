@@ -1,0 +1,12 @@
+#pragma once
+#include "kplex_common.h"
+
+namespace kplex {
+struct Prepped {
+    Csr g;                       // pruned graph, ids renumbered in ascending order
+    std::vector<int32_t> dpos;   // rank of each pruned vertex in the degeneracy order
+    std::vector<int32_t> dseq;   // pruned vertex at each rank
+    std::vector<uint32_t> orig;  // pruned id -> id in the input graph
+};
+int preprocess(const Csr& in, int k, int q, int truss, int threads, Prepped& out);
+}  // namespace kplex

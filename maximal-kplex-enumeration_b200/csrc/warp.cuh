@@ -1,0 +1,150 @@
+// Warp-level building blocks: reductions, scans, bitset <-> list conversion and
+// the task pool (a bounded multi-producer multi-consumer ring whose slots carry
+// sequence numbers, after D. Vyukov's published bounded MPMC queue).
+#pragma once
+#include "device.cuh"
+
+namespace kplex {
+
+constexpr unsigned FULL = 0xffffffffu;
+
+__device__ __forceinline__ int warp_sum(int v) {
+#pragma unroll
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+    return v;
+}
+__device__ __forceinline__ unsigned warp_min(unsigned v) {
+#pragma unroll
+    for (int o = 16; o; o >>= 1) v = min(v, __shfl_xor_sync(FULL, v, o));
+    return v;
+}
+__device__ __forceinline__ unsigned warp_or(unsigned v) {
+#pragma unroll
+    for (int o = 16; o; o >>= 1) v |= __shfl_xor_sync(FULL, v, o);
+    return v;
+}
+// exclusive prefix sum across the warp; *total receives the sum
+__device__ __forceinline__ int warp_excl_scan(int v, int* total) {
+    const unsigned l = lane_id();
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(FULL, x, o);
+        if ((int)l >= o) x += y;
+    }
+    *total = __shfl_sync(FULL, x, 31);
+    return x - v;
+}
+
+// Lane l holds word l of a bitset (0 beyond its length).  Writes the set
+// bits' indices in ascending order to list[0..) and returns their count.
+__device__ __forceinline__ int bits_to_list(unsigned w, uint16_t* list) {
+    const unsigned l = lane_id();
+    int tot;
+    int off = warp_excl_scan(__popc(w), &tot);
+    while (w) {
+        const int b = __ffs(w) - 1;
+        list[off++] = (uint16_t)(l * 32 + b);
+        w &= w - 1;
+    }
+    __syncwarp();
+    return tot;
+}
+
+__device__ __forceinline__ bool test_bit(const uint32_t* bits, unsigned v) { return (bits[v >> 5] >> (v & 31)) & 1u; }
+
+// popcount of (row & mask) over W words (W a multiple of 4, row 16-byte aligned)
+__device__ __forceinline__ int row_and_popc(const uint32_t* __restrict__ row, const uint32_t* mask, unsigned W) {
+    int c = 0;
+    const uint4* r4 = reinterpret_cast<const uint4*>(row);
+    const uint4* m4 = reinterpret_cast<const uint4*>(mask);
+    for (unsigned w = 0; w < W / 4; ++w) {
+        const uint4 a = __ldg(r4 + w), m = m4[w];
+        c += __popc(a.x & m.x) + __popc(a.y & m.y) + __popc(a.z & m.z) + __popc(a.w & m.w);
+    }
+    return c;
+}
+
+// ---------------------------------------------------------------- task pool
+// Enqueue one record (slot_words words, lane l supplies words l, l+32, ...
+// through `word(i)`).  Returns false when the ring is full or the bounded
+// retry loop gives up; the caller keeps the record.
+template <typename WordFn>
+__device__ inline bool pool_push(const SearchParams& sp, WordFn word) {
+    Pool* pool = sp.pool;
+    const unsigned l = lane_id();
+    unsigned long long pos = 0;
+    int ok = 0;
+    if (l == 0) {
+        const unsigned long long cap = pool->cap;
+        for (unsigned long long it = 0; it < sp.spin_limit; ++it) {
+            pos = atomicAdd(&pool->tail, 0ull);
+            const uint32_t seq = atomicAdd(&sp.pool_seq[pos % cap], 0u);
+            const int dif = (int)(seq - (uint32_t)pos);
+            if (dif == 0) {
+                if (atomicCAS(&pool->tail, pos, pos + 1) == pos) { ok = 1; break; }
+            } else if (dif < 0) {
+                break;   // full
+            }
+        }
+    }
+    ok = __shfl_sync(FULL, ok, 0);
+    if (!ok) return false;
+    pos = __shfl_sync(FULL, pos, 0);
+    const unsigned long long slot = pos % pool->cap;
+    uint32_t* dst = sp.pool_data + slot * sp.slot_words;
+    for (unsigned i = l; i < sp.slot_words; i += 32) __stcg(dst + i, word(i));
+    __threadfence();
+    __syncwarp();
+    if (l == 0) atomicExch(&sp.pool_seq[slot], (uint32_t)(pos + 1));
+    return true;
+}
+
+// Dequeue one record into dst (smem or gmem, slot_words words).  Returns
+// false if the ring looks empty (a record still being published counts as empty).
+__device__ inline bool pool_pop(const SearchParams& sp, uint32_t* dst) {
+    Pool* pool = sp.pool;
+    const unsigned l = lane_id();
+    unsigned long long pos = 0;
+    int ok = 0;
+    if (l == 0) {
+        const unsigned long long cap = pool->cap;
+        for (unsigned long long it = 0; it < sp.spin_limit; ++it) {
+            pos = atomicAdd(&pool->head, 0ull);
+            const uint32_t seq = atomicAdd(&sp.pool_seq[pos % cap], 0u);
+            const int dif = (int)(seq - (uint32_t)(pos + 1));
+            if (dif == 0) {
+                if (atomicCAS(&pool->head, pos, pos + 1) == pos) { ok = 1; break; }
+            } else if (dif < 0) {
+                break;   // empty
+            }
+        }
+    }
+    ok = __shfl_sync(FULL, ok, 0);
+    if (!ok) return false;
+    pos = __shfl_sync(FULL, pos, 0);
+    const unsigned long long cap = pool->cap;
+    const unsigned long long slot = pos % cap;
+    __threadfence();
+    const uint32_t* src = sp.pool_data + slot * sp.slot_words;
+    for (unsigned i = l; i < sp.slot_words; i += 32) dst[i] = __ldcg(src + i);
+    __threadfence();
+    __syncwarp();
+    if (l == 0) atomicExch(&sp.pool_seq[slot], (uint32_t)(pos + cap));
+    return true;
+}
+
+__device__ __forceinline__ unsigned long long pool_size(const SearchParams& sp) {
+    const unsigned long long t = *(volatile unsigned long long*)&sp.pool->tail;
+    const unsigned long long h = *(volatile unsigned long long*)&sp.pool->head;
+    return t > h ? t - h : 0ull;
+}
+
+// pool_size read once by lane 0 and broadcast, so every lane takes the same branch
+__device__ __forceinline__ unsigned long long pool_size_warp(const SearchParams& sp) {
+    unsigned long long v = 0;
+    if (lane_id() == 0) v = pool_size(sp);
+    return __shfl_sync(FULL, v, 0);
+}
+
+}  // namespace kplex

@@ -1,0 +1,245 @@
+"""Python view of libkplex.so (include/kplex.h) for tests, the bench and scripting.
+
+The product is the C ABI; this module only marshals numpy arrays into it.  It
+mirrors the reference's drop-in surface: `enumerate_file(path, k, q, t, truss)`
+is `./main <graph> -k K -q Q -t T -tr TR` (main.cu:11-61) and returns the
+values the reference prints (inc/host_funcs.h:1149-1157) plus the 64-bit
+count and the plex hash.  There is no CPU fallback: if libkplex.so is missing
+or no sm_100 device is present, the calls fail with KplexError.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libkplex.so")
+
+OK, ERR_PARAM, ERR_IO, ERR_FORMAT, ERR_CUDA, ERR_NOMEM, ERR_CAPACITY, ERR_TIMEOUT, ERR_NO_DEVICE, ERR_INTERNAL = range(10)
+FLAG_QUIET, FLAG_NO_HASH, FLAG_FORCE_SPILL, FLAG_TEST_NO_WAIT = 0x1, 0x2, 0x4, 0x8
+
+
+class KplexError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"kplex status {status}: {message}")
+        self.status = status
+
+
+class Params(ctypes.Structure):
+    _fields_ = [("k", ctypes.c_int), ("q", ctypes.c_int), ("thres", ctypes.c_float), ("truss", ctypes.c_int),
+                ("flags", ctypes.c_uint32), ("device", ctypes.c_int), ("pool_slots", ctypes.c_uint64),
+                ("omp_threads", ctypes.c_uint32), ("shard_index", ctypes.c_uint32), ("shard_count", ctypes.c_uint32)]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [("count", ctypes.c_uint64), ("hash", ctypes.c_uint64), ("valid_roots", ctypes.c_uint64),
+                ("tasks", ctypes.c_uint64), ("nodes", ctypes.c_uint64), ("pn", ctypes.c_uint32), ("pm", ctypes.c_uint32),
+                ("max_local_n", ctypes.c_uint32), ("max_left", ctypes.c_uint32), ("pauses", ctypes.c_uint32),
+                ("spilled", ctypes.c_uint32), ("ms_preprocess", ctypes.c_double), ("ms_device", ctypes.c_double),
+                ("ms_ref_region", ctypes.c_double), ("ms_total", ctypes.c_double), ("status", ctypes.c_int),
+                ("gpu_launches", ctypes.c_uint32), ("ms_decompose", ctypes.c_double), ("ms_ksearch", ctypes.c_double),
+                ("ms_bnb", ctypes.c_double), ("bnb_bytes", ctypes.c_uint64), ("roots_bytes", ctypes.c_uint64)]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class Graph(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_uint32), ("m_directed", ctypes.c_uint64),
+                ("offsets", ctypes.POINTER(ctypes.c_uint32)), ("neighbors", ctypes.POINTER(ctypes.c_uint32))]
+
+
+class GenSpec(ctypes.Structure):
+    _fields_ = [("seed", ctypes.c_uint64), ("n", ctypes.c_uint32), ("base_edges", ctypes.c_uint64),
+                ("exponent", ctypes.c_double), ("max_degree", ctypes.c_uint32), ("groups", ctypes.c_uint32),
+                ("group_min", ctypes.c_uint32), ("group_max", ctypes.c_uint32),
+                ("density_min", ctypes.c_double), ("density_max", ctypes.c_double)]
+
+
+# The benchmark workloads (seeded synthetic stand-ins for the reference's inputs).
+WORKLOADS = {
+    # Chung-Lu n=2,000, mean degree 10, exponent 2.5, 20 planted groups of 16 at density 0.9; k=2 q=8
+    "small": dict(spec=dict(seed=1, n=2000, base_edges=10000, exponent=2.5, max_degree=0, groups=20,
+                            group_min=16, group_max=16, density_min=0.9, density_max=0.9), k=2, q=8, thres=0.25, truss=0),
+    # epinions-shaped: n=75,879, 405,740 edges, exponent 2.1, cap 3,044, 200 groups U[40,80] at 0.9; k=4 q=30
+    "epinions": dict(spec=dict(seed=2, n=75879, base_edges=405740, exponent=2.1, max_degree=3044, groups=200,
+                               group_min=40, group_max=80, density_min=0.9, density_max=0.9), k=4, q=30, thres=0.25, truss=0),
+    # email-euall-shaped: n=265,214, 364,481 edges, exponent 1.8, cap 7,636, 50 groups U[15,25] at 0.85; k=3 q=12, truss
+    "email": dict(spec=dict(seed=3, n=265214, base_edges=364481, exponent=1.8, max_degree=7636, groups=50,
+                            group_min=15, group_max=25, density_min=0.85, density_max=0.85), k=3, q=12, thres=0.25, truss=1),
+}
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise KplexError(ERR_NO_DEVICE, f"{LIB_PATH} is not built (run make in {HERE})")
+        L = ctypes.CDLL(LIB_PATH)
+        u32p = ctypes.POINTER(ctypes.c_uint32)
+        L.kplex_enumerate_csr.argtypes = [u32p, u32p, ctypes.c_uint32, ctypes.c_uint64, ctypes.POINTER(Params), ctypes.POINTER(Result)]
+        L.kplex_enumerate_file.argtypes = [ctypes.c_char_p, ctypes.POINTER(Params), ctypes.POINTER(Result)]
+        L.kplex_prepare.argtypes = [u32p, u32p, ctypes.c_uint32, ctypes.c_uint64, ctypes.POINTER(Params),
+                                    ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(Result)]
+        L.kplex_search.argtypes = [ctypes.c_void_p, ctypes.POINTER(Result)]
+        L.kplex_release.argtypes = [ctypes.c_void_p]
+        L.kplex_release.restype = None
+        L.kplex_load_bin.argtypes = [ctypes.c_char_p, ctypes.POINTER(Graph)]
+        L.kplex_save_bin.argtypes = [ctypes.c_char_p, ctypes.POINTER(Graph)]
+        L.kplex_free_graph.argtypes = [ctypes.POINTER(Graph)]
+        L.kplex_free_graph.restype = None
+        L.kplex_generate.argtypes = [ctypes.POINTER(GenSpec), ctypes.POINTER(Graph)]
+        L.kplex_status_string.restype = ctypes.c_char_p
+        L.kplex_last_error.restype = ctypes.c_char_p
+        L.kplex_device_ok.argtypes = [ctypes.c_int]
+        i32p = ctypes.POINTER(ctypes.c_int32)
+        L.kplex_preprocess_csr.argtypes = [u32p, u32p, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int, ctypes.c_int,
+                                           ctypes.c_int, ctypes.c_uint32, u32p, u32p, i32p, i32p, u32p,
+                                           ctypes.POINTER(ctypes.c_uint64)]
+        L.kplex_preprocess_csr.restype = ctypes.c_longlong
+        _lib = L
+    return _lib
+
+
+def _err(status: int) -> KplexError:
+    L = lib()
+    return KplexError(status, f"{L.kplex_status_string(status).decode()}: {L.kplex_last_error().decode()}")
+
+
+def _u32p(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32))
+
+
+def _graph_to_numpy(g: Graph):
+    off = np.ctypeslib.as_array(g.offsets, shape=(g.n + 1,)).copy()
+    adj = np.ctypeslib.as_array(g.neighbors, shape=(max(g.m_directed, 1),))[: g.m_directed].copy()
+    return off, adj
+
+
+def load_bin(path: str):
+    """Read a reference .bin graph; returns (offsets u32[n+1], neighbors u32[m])."""
+    g = Graph()
+    rc = lib().kplex_load_bin(path.encode(), ctypes.byref(g))
+    if rc:
+        raise _err(rc)
+    try:
+        return _graph_to_numpy(g)
+    finally:
+        lib().kplex_free_graph(ctypes.byref(g))
+
+
+def save_bin(path: str, off: np.ndarray, adj: np.ndarray) -> None:
+    off = np.ascontiguousarray(off, dtype=np.uint32)
+    adj = np.ascontiguousarray(adj, dtype=np.uint32)
+    g = Graph(len(off) - 1, len(adj), _u32p(off), _u32p(adj))
+    rc = lib().kplex_save_bin(path.encode(), ctypes.byref(g))
+    if rc:
+        raise _err(rc)
+
+
+def generate(spec: dict):
+    """Seeded synthetic graph (see WORKLOADS); returns (offsets, neighbors)."""
+    s = GenSpec(**spec)
+    g = Graph()
+    rc = lib().kplex_generate(ctypes.byref(s), ctypes.byref(g))
+    if rc:
+        raise _err(rc)
+    try:
+        return _graph_to_numpy(g)
+    finally:
+        lib().kplex_free_graph(ctypes.byref(g))
+
+
+def workload_graph(name: str):
+    return generate(WORKLOADS[name]["spec"])
+
+
+def make_params(k: int, q: int, thres: float = 0.25, truss: int = 0, flags: int = FLAG_QUIET, device: int = 0,
+                pool_slots: int = 0, omp_threads: int = 0, shard_index: int = 0, shard_count: int = 0) -> Params:
+    return Params(k, q, thres, truss, flags, device, pool_slots, omp_threads, shard_index, shard_count)
+
+
+def enumerate_csr(off: np.ndarray, adj: np.ndarray, k: int, q: int, thres: float = 0.25, truss: int = 0,
+                  flags: int = FLAG_QUIET, device: int = 0, pool_slots: int = 0, check: bool = True,
+                  shard_index: int = 0, shard_count: int = 0) -> dict:
+    off = np.ascontiguousarray(off, dtype=np.uint32)
+    adj = np.ascontiguousarray(adj, dtype=np.uint32)
+    p = make_params(k, q, thres, truss, flags, device, pool_slots, 0, shard_index, shard_count)
+    r = Result()
+    rc = lib().kplex_enumerate_csr(_u32p(off), _u32p(adj), len(off) - 1, len(adj), ctypes.byref(p), ctypes.byref(r))
+    if rc and check:
+        raise _err(rc)
+    return r.as_dict()
+
+
+def enumerate_file(path: str, k: int, q: int, thres: float = 0.25, truss: int = 0, flags: int = FLAG_QUIET,
+                   device: int = 0) -> dict:
+    p = make_params(k, q, thres, truss, flags, device)
+    r = Result()
+    rc = lib().kplex_enumerate_file(path.encode(), ctypes.byref(p), ctypes.byref(r))
+    if rc:
+        raise _err(rc)
+    return r.as_dict()
+
+
+@dataclass
+class Prepared:
+    """Preprocessed graph resident on the device; search() reruns the device stage."""
+    handle: ctypes.c_void_p
+    pre: dict
+
+    def search(self) -> dict:
+        r = Result()
+        rc = lib().kplex_search(self.handle, ctypes.byref(r))
+        if rc:
+            raise _err(rc)
+        return r.as_dict()
+
+    def release(self) -> None:
+        if self.handle:
+            lib().kplex_release(self.handle)
+            self.handle = None
+
+
+def prepare(off: np.ndarray, adj: np.ndarray, k: int, q: int, thres: float = 0.25, truss: int = 0,
+            flags: int = FLAG_QUIET, device: int = 0, pool_slots: int = 0, shard_index: int = 0,
+            shard_count: int = 0) -> Prepared:
+    off = np.ascontiguousarray(off, dtype=np.uint32)
+    adj = np.ascontiguousarray(adj, dtype=np.uint32)
+    p = make_params(k, q, thres, truss, flags, device, pool_slots, 0, shard_index, shard_count)
+    h = ctypes.c_void_p()
+    r = Result()
+    rc = lib().kplex_prepare(_u32p(off), _u32p(adj), len(off) - 1, len(adj), ctypes.byref(p), ctypes.byref(h), ctypes.byref(r))
+    if rc:
+        raise _err(rc)
+    return Prepared(h, r.as_dict())
+
+
+def preprocess(off: np.ndarray, adj: np.ndarray, k: int, q: int, truss: int = 0, omp_threads: int = 0) -> dict:
+    """Host preprocessing only: pruned CSR, degeneracy order, pruned->input id map."""
+    off = np.ascontiguousarray(off, dtype=np.uint32)
+    adj = np.ascontiguousarray(adj, dtype=np.uint32)
+    n = len(off) - 1
+    o_off = np.zeros(n + 1, dtype=np.uint32)
+    o_adj = np.zeros(max(len(adj), 1), dtype=np.uint32)
+    o_dpos = np.zeros(max(n, 1), dtype=np.int32)
+    o_dseq = np.zeros(max(n, 1), dtype=np.int32)
+    o_orig = np.zeros(max(n, 1), dtype=np.uint32)
+    m = ctypes.c_uint64()
+    i32 = ctypes.POINTER(ctypes.c_int32)
+    pn = lib().kplex_preprocess_csr(_u32p(off), _u32p(adj), n, len(adj), k, q, truss, omp_threads, _u32p(o_off),
+                                    _u32p(o_adj), o_dpos.ctypes.data_as(i32), o_dseq.ctypes.data_as(i32),
+                                    _u32p(o_orig), ctypes.byref(m))
+    if pn < 0:
+        raise _err(int(-pn))
+    return {"pn": int(pn), "off": o_off[: pn + 1], "adj": o_adj[: m.value], "dpos": o_dpos[:pn], "dseq": o_dseq[:pn],
+            "orig": o_orig[:pn]}
+
+
+def device_ok(device: int = 0) -> bool:
+    return bool(lib().kplex_device_ok(device))
