@@ -1,0 +1,297 @@
+#!/usr/bin/env python
+"""Benchmark: maximal k-plexes per second on B200 (one JSON line on rank 0).
+
+One step = one full enumeration of the workload graph on the device
+(decomposition + k-search + branch-and-bound), with the pruned graph already
+resident in HBM (`value`), and the same enumeration through the public C ABI
+from host CSR arrays (`e2e`: host preprocessing, upload, search, result read).
+Under torchrun each rank searches the roots whose degeneracy rank r satisfies
+r % world == rank (strong scaling over one graph); the only collective is a
+final all-reduce of (count, hash, device time).
+
+--impl reference times the reference algorithm's CPU restatement (the oracle,
+OpenMP over all host cores) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "maximal-kplex-enumeration_b200")
+sys.path.insert(0, PKG)
+
+import numpy as np  # noqa: E402
+
+import kplex_b200 as kp  # noqa: E402
+
+METRIC = "maximal k-plexes/sec"
+UNIT = "plexes/s"
+
+
+def load_workload(name: str):
+    if name in kp.WORKLOADS:
+        w = kp.WORKLOADS[name]
+        off, adj = kp.workload_graph(name)
+        return off, adj, dict(workload=f"{name}-shaped synthetic" if name != "small" else "small synthetic",
+                              seed=w["spec"]["seed"], n=int(len(off) - 1), m_directed=int(len(adj)),
+                              k=w["k"], q=w["q"], t=w["thres"], truss=w["truss"])
+    # a real .bin graph: name = path:k:q:truss
+    path, k, q, tr = name.split(":")
+    off, adj = kp.load_bin(path)
+    return off, adj, dict(workload=os.path.basename(path), n=int(len(off) - 1), m_directed=int(len(adj)),
+                          k=int(k), q=int(q), t=0.25, truss=int(tr))
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown," \
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown," \
+             "clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+        self.t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict | None:
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.t:
+            self.t.join(timeout=2)
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def allreduce_results(dist, count: int, hsum: int, ms: float, device) -> tuple[int, int, float]:
+    """Whole-graph (count, hash) = sums over root shards (hash mod 2^64); time = max over ranks."""
+    import torch
+    mx = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+    signed = hsum - (1 << 64) if hsum >= (1 << 63) else hsum
+    tot = torch.tensor([count, signed], dtype=torch.int64, device=device)
+    dist.all_reduce(tot)
+    return int(tot[0].item()), int(tot[1].item()) & ((1 << 64) - 1), float(mx.item())
+
+
+def cpu_sample(off, adj, cfg, budget_s: float = 20.0):
+    """Oracle (OpenMP, all host cores) on a bounded root sample of the workload."""
+    sys.path.insert(0, ROOT)
+    import oracle  # CPU baseline only
+
+    pre = oracle.preprocess(off, adj, cfg["k"], cfg["q"], cfg["truss"])
+    nroots = max(0, pre["pn"] - cfg["q"] + 2)
+    # grow a contiguous range of the latest-ranked roots until the sample takes ~budget_s
+    span = max(1, nroots // 64)
+    best = None
+    while True:
+        b = max(0, nroots - span)
+        t0 = time.perf_counter()
+        r = oracle.enumerate_csr(off, adj, cfg["k"], cfg["q"], cfg["truss"], threads=0, root_begin=b, root_end=nroots)
+        el = time.perf_counter() - t0
+        best = (r, el, b, nroots)
+        if el >= budget_s / 4 or span >= nroots:
+            break
+        span = min(nroots, span * 4)
+    r, el, b, e = best
+    return {"value": r["count"] / el if el > 0 else 0.0, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+            "sample": f"roots of degeneracy rank [{b},{e}) of {nroots}: {r['count']} plexes in {el:.2f} s "
+                      f"(oracle restatement, all {os.cpu_count()} host threads)"}
+
+
+def run_reference(args, cfg, off, adj):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    steps = []
+    for i in range(args.warmup + args.steps):
+        cb = cpu_sample(off, adj, cfg, budget_s=args.cpu_budget)
+        if i >= args.warmup:
+            steps.append(cb)
+    v = statistics.median([s["value"] for s in steps])
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic (seeded Chung-Lu + planted dense groups)" if "synthetic" in cfg["workload"] else "file",
+            "config": cfg, "cpu_baseline": {**steps[-1], "value": v},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="epinions")
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    off, adj, cfg = load_workload(args.workload)
+    if args.impl == "reference":
+        run_reference(args, cfg, off, adj)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    cfg.update(parallelism=f"root-shard x{world}" if world > 1 else "single GPU",
+               l2="256 MiB flush between steps")
+    prep = kp.prepare(off, adj, cfg["k"], cfg["q"], cfg["t"], cfg["truss"], device=local,
+                      shard_index=rank if world > 1 else 0, shard_count=world if world > 1 else 0)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+    for _ in range(args.warmup):
+        prep.search()
+        flush.zero_()
+    barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    res = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        res.append(prep.search())
+    barrier()
+    clocks = sampler.stop()
+
+    dev_ms = sum(r["ms_device"] for r in res)
+    bnb_ms = sum(r["ms_bnb"] for r in res)
+    bnb_bytes = sum(r["bnb_bytes"] for r in res)
+    bnb_launches = sum(1 + r["pauses"] for r in res)
+    launches = sum(r["gpu_launches"] for r in res)
+    count = res[-1]["count"]
+    hsum = res[-1]["hash"]
+    consistent = all(r["count"] == count and r["hash"] == hsum for r in res)
+    if world > 1:
+        total_count, total_hash, dev_ms_max = allreduce_results(dist, count, hsum, dev_ms, f"cuda:{local}")
+    else:
+        dev_ms_max, total_count, total_hash = dev_ms, count, hsum
+
+    # end to end through the public C ABI from host CSR arrays (rank's shard)
+    e2e_ms = []
+    e2e_count = 0
+    for _ in range(args.e2e_steps):
+        r = kp.enumerate_csr(off, adj, cfg["k"], cfg["q"], cfg["t"], cfg["truss"], device=local,
+                             shard_index=rank if world > 1 else 0, shard_count=world if world > 1 else 0)
+        e2e_ms.append(r["ms_total"])
+        e2e_count = r["count"]
+    if world > 1:
+        e = torch.tensor([max(e2e_ms)], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(e, op=dist.ReduceOp.MAX)
+        e2e_max = float(e.item())
+        c = torch.tensor([e2e_count], dtype=torch.int64, device=f"cuda:{local}")
+        dist.all_reduce(c)
+        e2e_total = int(c.item())
+    else:
+        e2e_max, e2e_total = statistics.median(e2e_ms), e2e_count
+    pr = prep.pre
+    h2d = 4 * ((pr["pn"] + 1) + pr["pm"] + 3 * pr["pn"])
+
+    peak, peak_kind = measured_peak()
+    achieved = (bnb_bytes / (bnb_ms / 1e3)) / 1e9 if bnb_ms > 0 else 0.0
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "bnb_traffic.json")
+    if os.path.exists(prof):
+        with open(prof) as f:
+            pj = json.load(f)
+        if pj.get("workload") == args.workload:
+            traffic = pj.get("dram_bytes_per_launch")
+
+    line = {
+        "metric": METRIC,
+        "value": total_count * args.steps / (dev_ms_max / 1e3) if dev_ms_max > 0 else 0.0,
+        "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic (seeded Chung-Lu + planted dense groups)" if "synthetic" in cfg["workload"] else "file",
+        "config": cfg,
+        "count": total_count, "hash": f"{total_hash:#018x}", "results_consistent": consistent,
+        "roofline": {"bound": "hbm", "kernel": "bnb_kernel", "achieved": achieved, "peak": peak,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak if peak else 0.0,
+                     "traffic": traffic, "bytes_per_launch": bnb_bytes / max(bnb_launches, 1),
+                     "ms_per_launch": bnb_ms / max(bnb_launches, 1)},
+        "e2e": {"value": e2e_total / (e2e_max / 1e3) if e2e_max > 0 else 0.0, "unit": UNIT,
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 512, "ms_per_step": e2e_max},
+        "gpu_launches": launches,
+        "phases_ms_per_step": {"decompose": sum(r["ms_decompose"] for r in res) / args.steps,
+                               "ksearch": sum(r["ms_ksearch"] for r in res) / args.steps,
+                               "bnb": bnb_ms / args.steps},
+        "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_sample(off, adj, cfg, budget_s=args.cpu_budget)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    prep.release()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

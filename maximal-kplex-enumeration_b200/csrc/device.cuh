@@ -71,6 +71,8 @@ struct Counters {
     unsigned int decomp_next;      // decomposition root dispenser
     unsigned int pad[3];
     unsigned long long roots_bytes; // algorithmic bytes of the decomposition
+    unsigned long long ks_tasks;   // tasks emitted by k-search
+    unsigned int stuck_once;       // test hook: one pool slot claimed and never published
 };
 
 // Vyukov bounded MPMC ring: each slot carries a sequence number so that a
@@ -110,6 +112,7 @@ struct SearchParams {
     uint32_t low_water;        // a branch warp donates work when the pool holds fewer records
     uint32_t hash_on;
     uint32_t shard_index, shard_count;
+    uint32_t test_stuck;       // test hook: the first push claims a slot and never publishes it
     unsigned long long spin_limit;   // iterations for any bounded wait
 };
 

@@ -5,10 +5,11 @@
 // host:916-1011), launches five kernels per wave of 4,544 roots and reads a
 // flag back after every BNB wave (host:253-335).  Here one search is:
 //   decompose_kernel  all roots at once into a bump-allocated arena
-//   ksearch_kernel    fills the task pool until it holds thres * capacity records
-//   bnb_kernel        persistent; drains the pool with per-warp depth-first stacks
-//   (repeat k-search + branch while k-search paused: pause-and-resume, host:1094-1122)
-// with a handful of 64-byte counter reads in total.  Device buffers are cached
+//   search_kernel     persistent: producer warps run k-search into the task pool
+//                     (pausing on the device at thres * capacity records), consumer
+//                     warps drain it depth-first (pause-and-resume, host:1094-1122,
+//                     without a host round trip)
+// with two 128-byte counter reads in total.  Device buffers are cached
 // per device and grown on demand.
 #include <cuda_runtime.h>
 
@@ -28,8 +29,7 @@
 namespace kplex {
 
 __global__ void decompose_kernel(SearchParams sp);
-__global__ void ksearch_kernel(SearchParams sp);
-__global__ void bnb_kernel(SearchParams sp, uint32_t nmax);
+__global__ void search_kernel(SearchParams sp, uint32_t nmax);
 uint64_t decomp_scratch_words_host(uint32_t pn);
 uint32_t bnb_smem_words_host(uint32_t nmax, uint32_t slot_words);
 uint32_t ks_slot_words_host();
@@ -275,48 +275,34 @@ static int search_impl(kplex_prepared* h, kplex_result* out) {
     sp.pool_data = d->pool_data.as<uint32_t>();
     init_pool<<<d->sms * 4, 256, 0, st>>>(sp.pool_seq, cap, sp.pool);
     ++launches;
-    const uint32_t ks_warps = (uint32_t)d->sms * 8;
-    if ((rc = d->ks.ensure((size_t)ks_warps * ks_slot_words_host() * 4))) return rc;
-    sp.ks_slots = d->ks.as<uint32_t>();
-    init_ks_slots<<<(ks_warps + 255) / 256, 256, 0, st>>>(sp.ks_slots, ks_warps, ks_slot_words_host());
-    ++launches;
-    const long long pause = (long long)std::floor((double)cap * (double)P.thres) - (long long)ks_warps;   // host:2083 MAX_CAP*thres - WARPS
-    sp.pause_at = (unsigned long long)std::max<long long>(pause, 1);
-
-    const uint32_t smem_words = bnb_smem_words_host(nmax, sp.slot_words);
+    const uint32_t smem_words = ks_slot_words_host() + 8 * bnb_smem_words_host(nmax, sp.slot_words);
     const int warps_per_block = 8;
-    const size_t smem_bytes = (size_t)smem_words * 4 * warps_per_block;
-    CK(cudaFuncSetAttribute(bnb_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes));
+    const size_t smem_bytes = (size_t)smem_words * 4;
+    CK(cudaFuncSetAttribute(search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes));
     int per_sm = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bnb_kernel, warps_per_block * 32, smem_bytes));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, search_kernel, warps_per_block * 32, smem_bytes));
     per_sm = std::max(per_sm, 1);
-    const uint32_t bnb_blocks = (uint32_t)d->sms * (uint32_t)per_sm;
-    const uint32_t bnb_warps = bnb_blocks * warps_per_block;
-    sp.nwarps = bnb_warps;
+    const uint32_t blocks = (uint32_t)d->sms * (uint32_t)per_sm;
+    const uint32_t nwarps = blocks * warps_per_block;
+    sp.nwarps = nwarps;
     sp.stack_depth = nmax + 2;
-    sp.low_water = 2 * bnb_warps;
-    if ((rc = d->stacks.ensure((size_t)bnb_warps * sp.stack_depth * sp.slot_words * 4))) return rc;
+    sp.low_water = 2 * nwarps;
+    // the reference pauses at MAX_CAP * thres - WARPS (src:2083, 2384): one record of slack per producer
+    const long long pause = (long long)std::floor((double)cap * (double)P.thres) - (long long)blocks;
+    sp.pause_at = (unsigned long long)std::max<long long>(pause, 1);
+    if ((rc = d->stacks.ensure((size_t)nwarps * sp.stack_depth * sp.slot_words * 4))) return rc;
     sp.stacks = d->stacks.as<uint32_t>();
-
-    // ---------------- k-search / branch-and-bound with pause-and-resume
-    uint32_t pauses = 0;
-    for (int cycle = 0;; ++cycle) {
-        if (cycle > (1 << 22)) { g_last_error = "pause-and-resume did not finish"; return KPLEX_ERR_INTERNAL; }
-        CK(cudaMemsetAsync(&sp.ctr->ks_paused, 0, sizeof(unsigned), st));
-        if (nroots) {
-            if ((rc = timed([&] { ksearch_kernel<<<ks_warps / 4, 128, 0, st>>>(sp); }, ms_ks))) return rc;
-            ++launches;
-            SearchParams sb = sp;
-            if (P.flags & KPLEX_FLAG_TEST_NO_WAIT) sb.spin_limit = 0;   // failure-detection test hook
-            if ((rc = timed([&] { bnb_kernel<<<bnb_blocks, warps_per_block * 32, smem_bytes, st>>>(sb, nmax); }, ms_bnb))) return rc;
-            ++launches;
-        }
-        CK(cudaMemcpyAsync(&hc, sp.ctr, sizeof(Counters), cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
-        if (hc.error) break;
-        if (hc.ks_paused == 0) break;
-        ++pauses;
+    if (P.flags & KPLEX_FLAG_TEST_NO_WAIT) {   // failure-detection test hook
+        sp.test_stuck = 1;
+        sp.spin_limit = 1u << 14;
     }
+
+    // ---------------- k-search + branch-and-bound, one persistent launch
+    if (nroots) {
+        if ((rc = timed([&] { search_kernel<<<blocks, warps_per_block * 32, smem_bytes, st>>>(sp, nmax); }, ms_bnb))) return rc;
+        ++launches;
+    }
+    CK(cudaMemcpyAsync(&hc, sp.ctr, sizeof(Counters), cudaMemcpyDeviceToHost, st));
     Pool hp;
     CK(cudaMemcpyAsync(&hp, sp.pool, sizeof(Pool), cudaMemcpyDeviceToHost, st));
     CK(cudaEventRecord(e1, st));
@@ -327,6 +313,7 @@ static int search_impl(kplex_prepared* h, kplex_result* out) {
     cudaEventDestroy(e1);
     cudaEventDestroy(ka);
     cudaEventDestroy(kb);
+    const uint32_t pauses = hc.ks_paused;
     if (!hc.error && hp.head != hp.tail) { hc.error = KPLEX_ERR_TIMEOUT; g_last_error = "branch warps gave up with records left in the pool"; }
     if (out) {
         out->count = hc.count;

@@ -12,8 +12,10 @@
 
 static void usage() { fprintf(stderr, "usage : ./PlexEnum <dataset> -k <k> -q <q> -t <thres> -tr <truss>\n"); }
 
+// main.cu:16-21 tests i == max before incrementing, so a flag in last position
+// reads argv[argc] (NULL) and aborts; here it is a usage error (exit 1).
 static int check_inc(int i, int max) {
-    if (i == max) { usage(); exit(1); }
+    if (i + 1 >= max) { usage(); exit(1); }
     return i + 1;
 }
 

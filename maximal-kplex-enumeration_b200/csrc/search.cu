@@ -1,21 +1,26 @@
-// k-search over C2 and task-based branch-and-bound.
+// k-search over C2 and task-based branch-and-bound in one persistent kernel.
 //
-// ksearch_kernel restates kSearch (src/device_funcs.cu:1855-2444): an explicit
-// stack of frames (res, br, state, v2delete) enumerates subsets of C2 of size
-// <= k-1; each leaf becomes one branch-and-bound task pushed into the shared
-// pool (the reference's queue A).  C1, X and P are bitsets held one word per
-// lane; the C2 list keeps the reference's order (pop_back / push_back /
-// ascending recovery, src:1124-1195) because that order decides which
-// subsets land in which branch.  When the pool holds `pause_at` records the
-// warp stops (state already in its slot) and the host drains the pool with
-// the branch kernel before relaunching it (pause-and-resume, host:1094-1122).
+// Reference structure (src/device_funcs.cu, inc/host_funcs.h): kSearch
+// (src:1855-2444) fills queue A with tasks, pausing when A holds
+// thres * MAX_CAP - WARPS records; the host then drains A with waves of the
+// BNB kernel (src:1516-1724) through auxiliary queues B and C (host:253-335),
+// reading a flag back after every wave, and relaunches kSearch (host:1094-1122).
 //
-// bnb_kernel restates BNB (src:1516-1724) with enqueue_exclude_child /
-// enqueue_include_child (src:1197-1465) as a persistent kernel: every warp
-// owns a depth-first stack of task records, continues with the include child
-// and stacks the exclude child, and donates its oldest record to the pool when
-// the pool runs low.  neiInG / neiInP (stored per task in the reference) are
-// recomputed from the bitsets: neiInG[v] = |N(v) ∩ (P ∪ C)|, neiInP[v] = |N(v) ∩ P|.
+// Here both run inside search_kernel:
+//  * warp 0 of every block is a producer: it claims roots and runs the k-search
+//    state machine with its whole state in shared memory.  Each leaf is one
+//    task (P, C, X bitsets) pushed into the pool, a bounded lock-free ring in
+//    HBM (the reference's queue A).  When the pool holds pause_at records the
+//    producer pauses and works as a consumer until the pool drains below
+//    half of that, then resumes (pause-and-resume without a host round trip).
+//    A push that finds the ring full is kept and processed by the producer.
+//  * the other warps are consumers: each pops a record and runs the branch
+//    and bound on it depth-first, continuing with the include child and
+//    stacking the exclude child in its own stack, and gives its oldest stacked
+//    record back to the pool when the pool runs low (load balancing that the
+//    reference gets from its queues B and C).
+// neiInG / neiInP, which the reference stores per task (u16 arrays, common.h:144-170),
+// are recomputed from the bitsets: neiInG[v] = |N(v) ∩ (P ∪ C)|, neiInP[v] = |N(v) ∩ P|.
 #include "warp.cuh"
 #include <climits>
 
@@ -48,18 +53,19 @@ __device__ __forceinline__ RootView root_view(const SearchParams& sp, uint32_t r
     return v;
 }
 
-// ============================================================== k-search
-// slot layout (words)
-constexpr int KS_HDR = 8;   // root, sz, np, nc2, active, pad...
-constexpr int KS_P = KS_HDR;                  // MAX_K words: P stack (local ids)
-constexpr int KS_FR = KS_P + MAX_K;           // KS_MAX_DEPTH + 1 frames
-constexpr int KS_C2 = KS_FR + KS_MAX_DEPTH + 8;   // MAX_LOCAL u16
-constexpr int KS_T1 = KS_C2 + MAX_LOCAL / 2;      // MAX_LOCAL u16 tags (C1)
-constexpr int KS_T2 = KS_T1 + MAX_LOCAL / 2;      // MAX_LOCAL u16 tags (C2)
-constexpr int KS_BITS = KS_T2 + MAX_LOCAL / 2;    // C1, X, P bitsets (3 * 32 words)
-constexpr int KS_WORDS = KS_BITS + 3 * MAX_WORDS;
+// ============================================================== k-search state (shared memory)
+constexpr int KS_HDR = 8;                         // root, sz, np, nc2
+constexpr int KS_P = KS_HDR;                      // MAX_K words: P stack (local ids, inclusion order)
+constexpr int KS_FR = KS_P + MAX_K;               // KS_MAX_DEPTH frames (+ slack)
+constexpr int KS_C2 = KS_FR + KS_MAX_DEPTH + 8;   // MAX_LOCAL u16: C2 list in the reference's order
+constexpr int KS_T1 = KS_C2 + MAX_LOCAL / 2;      // MAX_LOCAL u16: drop tags of C1 (depth + 1)
+constexpr int KS_T2 = KS_T1 + MAX_LOCAL / 2;      // MAX_LOCAL u16: drop tags of C2
+constexpr int KS_LST = KS_T2 + MAX_LOCAL / 2;     // MAX_LOCAL u16: C1 members (isKplex2 filter)
+constexpr int KS_BITS = KS_LST + MAX_LOCAL / 2;   // C1, X, P bitsets (32 words each)
+constexpr int KS_AUX = KS_BITS + 3 * MAX_WORDS;   // three 32-word scratch masks
+constexpr int KS_WORDS = KS_AUX + 3 * MAX_WORDS;
 
-// frame: res (8) | br (8) | state (4) | v2d (11)
+// frame: res (8) | br (8) | state (4) | v2delete (12)
 __device__ __forceinline__ uint32_t fr_pack(uint32_t res, uint32_t br, uint32_t st, uint32_t v) {
     return res | (br << 8) | (st << 16) | (v << 20);
 }
@@ -70,295 +76,242 @@ __device__ __forceinline__ uint32_t fr_v(uint32_t f) { return f >> 20; }
 
 struct KsSlot {
     uint32_t* w;
-    __device__ uint32_t& root() { return w[0]; }
-    __device__ uint32_t& sz() { return w[1]; }
-    __device__ uint32_t& np() { return w[2]; }
-    __device__ uint32_t& nc2() { return w[3]; }
-    __device__ uint32_t* P() { return w + KS_P; }
-    __device__ uint32_t* fr() { return w + KS_FR; }
-    __device__ uint16_t* c2() { return reinterpret_cast<uint16_t*>(w + KS_C2); }
-    __device__ uint16_t* t1() { return reinterpret_cast<uint16_t*>(w + KS_T1); }
-    __device__ uint16_t* t2() { return reinterpret_cast<uint16_t*>(w + KS_T2); }
-    __device__ uint32_t* bits() { return w + KS_BITS; }
+    __device__ uint32_t& root() const { return w[0]; }
+    __device__ uint32_t& sz() const { return w[1]; }
+    __device__ uint32_t& np() const { return w[2]; }
+    __device__ uint32_t& nc2() const { return w[3]; }
+    __device__ uint32_t* P() const { return w + KS_P; }
+    __device__ uint32_t* fr() const { return w + KS_FR; }
+    __device__ uint16_t* c2() const { return reinterpret_cast<uint16_t*>(w + KS_C2); }
+    __device__ uint16_t* t1() const { return reinterpret_cast<uint16_t*>(w + KS_T1); }
+    __device__ uint16_t* t2() const { return reinterpret_cast<uint16_t*>(w + KS_T2); }
+    __device__ uint16_t* lst() const { return reinterpret_cast<uint16_t*>(w + KS_LST); }
+    __device__ uint32_t* bits() const { return w + KS_BITS; }
+    __device__ uint32_t* mask() const { return w + KS_AUX; }
+    __device__ uint32_t* aux() const { return w + KS_AUX + MAX_WORDS; }
+    __device__ uint32_t* keep() const { return w + KS_AUX + 2 * MAX_WORDS; }
 };
 
-// neiInG of every P member against P ∪ C1 (upperBoundK2, src:1002-1020)
-__device__ bool ks_upper_bound(const SearchParams& sp, const RootView& R, KsSlot& S, uint32_t np, uint32_t PC1w, uint32_t* s_mask) {
+// Initial sets for root r (src:447-460, 1953-1975): P = {0}, C1 = [1,hop), C2 = [hop,n), X = {}.
+__device__ void ks_start(const SearchParams& sp, const KsSlot& S, uint32_t r, const RootDesc& d) {
     const unsigned l = lane_id();
-    s_mask[l] = PC1w;
+    const uint32_t n = d.n, hop = d.hop;
+    const uint32_t lo = l * 32;
+    uint32_t c1 = 0;
+    for (uint32_t b = 0; b < 32; ++b) { const uint32_t v = lo + b; if (v >= 1 && v < hop) c1 |= 1u << b; }
+    S.bits()[l] = c1;
+    S.bits()[MAX_WORDS + l] = 0u;
+    S.bits()[2 * MAX_WORDS + l] = (l == 0) ? 1u : 0u;
+    for (uint32_t i = l; i < n; i += 32) {
+        if (i >= hop) S.c2()[i - hop] = (uint16_t)i;
+        S.t1()[i] = 0;
+        S.t2()[i] = 0;
+    }
+    if (l == 0) {
+        S.P()[0] = 0;
+        S.np() = 1;
+        S.nc2() = n - hop;
+        S.sz() = 1;
+        S.fr()[0] = fr_pack((uint32_t)(sp.k - 1), 1, 0, 0);
+        S.root() = r;
+    }
+    __syncwarp();
+}
+
+// upperBoundK2 (src:1002-1020): every P member keeps neiInG + k >= q, neiInG over P ∪ C1.
+__device__ bool ks_upper_bound(const SearchParams& sp, const RootView& R, const KsSlot& S, uint32_t np, uint32_t PC1w) {
+    const unsigned l = lane_id();
+    S.mask()[l] = PC1w;
     __syncwarp();
     bool ok = true;
     for (uint32_t i = l; i < np; i += 32) {
         const uint32_t u = S.P()[i];
-        const int g = row_and_popc(R.A + (uint64_t)u * R.W, s_mask, R.W);
-        if (g + sp.k < sp.q) ok = false;
+        if (row_and_popc(R.A + (uint64_t)u * R.W, S.mask(), R.W) + sp.k < sp.q) ok = false;
     }
     ok = __all_sync(FULL, ok);
     __syncwarp();
     return ok;
 }
 
-__device__ __forceinline__ void write_task(const SearchParams& sp, uint32_t root, uint32_t np, uint32_t nc, uint32_t nx,
-                                           uint32_t Pw, uint32_t Cw, uint32_t Xw, uint32_t* dst) {
-    const unsigned l = lane_id();
-    const uint32_t Wt = sp.Wt;
-    if (l == 0) { dst[0] = root; dst[1] = np | (nc << 16); dst[2] = nx; dst[3] = 0; }
-    if (l < Wt) { dst[4 + l] = Pw; dst[4 + Wt + l] = Cw; dst[4 + 2 * Wt + l] = Xw; }
-}
+struct Emitted {
+    uint32_t np, nc, nx;
+    uint32_t Pw, Cw, Xw;   // this lane's word
+};
 
-__global__ void __launch_bounds__(128) ksearch_kernel(SearchParams sp) {
+// Runs the k-search state machine (src:1993-2442) of the root held in S until
+// it emits one task (returns 1, task in *e) or the root is finished (returns 0).
+// The frame bookkeeping after an emission is done before returning, so the
+// saved state resumes exactly where the reference resumes after its pause.
+__device__ int ks_advance(const SearchParams& sp, const KsSlot& S, Emitted* e) {
     const unsigned l = lane_id();
-    const unsigned warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    KsSlot S{sp.ks_slots + (uint64_t)warp * KS_WORDS};
-    __shared__ __align__(16) uint32_t s_mask_all[4][MAX_WORDS];
-    __shared__ __align__(16) uint32_t s_aux_all[4][MAX_WORDS];
-    uint32_t* s_mask = s_mask_all[threadIdx.x >> 5];
-    uint32_t* s_aux = s_aux_all[threadIdx.x >> 5];
     const int k = sp.k, q = sp.q;
-    unsigned long long tasks = 0;
+    const uint32_t r = S.root();
+    const RootView R = root_view(sp, r);
+    const uint32_t n = R.n, W = R.W;
+    uint32_t C1w = S.bits()[l], Xw = S.bits()[MAX_WORDS + l], Pw = S.bits()[2 * MAX_WORDS + l];
+    uint32_t sz = S.sz(), np = S.np(), nc2 = S.nc2();
+    int emitted = 0;
+    uint32_t emitC = 0;
 
-    for (;;) {
-        uint32_t r = S.root();
-        if (r == 0xffffffffu) {
-            if (pool_size_warp(sp) >= sp.pause_at) { if (l == 0) atomicAdd(&sp.ctr->ks_paused, 1u); break; }
-            if (l == 0) r = atomicAdd(&sp.ctr->next_root, 1u);
-            r = __shfl_sync(FULL, r, 0);
-            if (r >= sp.nroots) break;
-            const RootDesc d = sp.roots[r];
-            if (!(d.flags & ROOT_VALID) || d.n == 0) continue;
-            // initial sets (src:447-460, 1953-1975): P = {0}, C1 = [1,hop), C2 = [hop,n)
-            const uint32_t n = d.n, hop = d.hop;
-            uint32_t c1 = 0;
-            {
-                const uint32_t lo = l * 32;
-                for (uint32_t b = 0; b < 32; ++b) { const uint32_t v = lo + b; if (v >= 1 && v < hop) c1 |= 1u << b; }
+    auto update13 = [&](uint32_t node, uint16_t tag) {   // updateCand13, src:1042-1097
+        const uint32_t m2 = (l < W) ? __ldg(R.M2 + (uint64_t)node * W + l) : 0u;
+        uint32_t drop = C1w & ~m2;
+        C1w &= m2;
+        while (drop) { const int b = __ffs(drop) - 1; S.t1()[l * 32 + b] = tag; drop &= drop - 1; }
+    };
+    auto update23 = [&](uint32_t node, uint16_t tag) {   // updateCand23, src:1099-1122 (order preserving)
+        const uint32_t* m2row = R.M2 + (uint64_t)node * W;
+        uint32_t write = 0;
+        for (uint32_t b = 0; b < nc2; b += 32) {
+            const uint32_t i = b + l;
+            uint16_t v = 0;
+            bool keep = false;
+            if (i < nc2) { v = S.c2()[i]; keep = (__ldg(m2row + (v >> 5)) >> (v & 31)) & 1u; }
+            const unsigned km = __ballot_sync(FULL, keep);
+            __syncwarp();
+            if (i < nc2) {
+                if (keep) S.c2()[write + __popc(km & ((1u << l) - 1))] = v;
+                else S.t2()[v] = tag;
             }
-            S.bits()[l] = c1;
-            S.bits()[MAX_WORDS + l] = 0u;
-            S.bits()[2 * MAX_WORDS + l] = (l == 0) ? 1u : 0u;
-            for (uint32_t i = l; i < n; i += 32) {
-                if (i >= hop) S.c2()[i - hop] = (uint16_t)i;
-                S.t1()[i] = 0; S.t2()[i] = 0;
-            }
-            if (l == 0) {
-                S.P()[0] = 0;
-                S.np() = 1; S.nc2() = n - hop; S.sz() = 1;
-                S.fr()[0] = fr_pack((uint32_t)(k - 1), 1, 0, 0);
-                S.root() = r;
-            }
+            write += __popc(km);
             __syncwarp();
         }
-        const RootView R = root_view(sp, r);
-        const uint32_t n = R.n, W = R.W;
-        uint32_t C1w = S.bits()[l], Xw = S.bits()[MAX_WORDS + l], Pw = S.bits()[2 * MAX_WORDS + l];
-        uint32_t sz = S.sz(), np = S.np(), nc2 = S.nc2();
-        bool paused = false;
+        nc2 = write;
+    };
+    auto include = [&](uint32_t u) {
+        if (l == 0) S.P()[np] = u;
+        ++np;
+        if (l == (u >> 5)) Pw |= 1u << (u & 31);
+        __syncwarp();
+    };
+    auto c2_pop = [&]() -> uint32_t { --nc2; return S.c2()[nc2]; };
+    auto c2_push = [&](uint32_t u) { __syncwarp(); if (l == 0) S.c2()[nc2] = (uint16_t)u; ++nc2; __syncwarp(); };
+    auto setfr = [&](uint32_t f, uint32_t val) { __syncwarp(); if (l == 0) S.fr()[f] = val; __syncwarp(); };
 
-        // The record is assembled in the pool directly: lane l writes its words.
-        auto push_task = [&](uint32_t Cw) -> int {
-            const int nc = warp_sum(__popc(Cw));
-            const int nx = warp_sum(__popc(Xw));
-            Pool* pool = sp.pool;
-            unsigned long long pos = 0;
-            int ok = 0;
-            if (l == 0) {
-                const unsigned long long cap = pool->cap;
-                for (unsigned long long it = 0; it < sp.spin_limit; ++it) {
-                    pos = atomicAdd(&pool->tail, 0ull);
-                    const uint32_t seq = atomicAdd(&sp.pool_seq[pos % cap], 0u);
-                    const int dif = (int)(seq - (uint32_t)pos);
-                    if (dif == 0) { if (atomicCAS(&pool->tail, pos, pos + 1) == pos) { ok = 1; break; } }
-                    else if (dif < 0) break;
-                }
+    while (sz && !emitted) {
+        if (sz >= (uint32_t)KS_MAX_DEPTH) {   // src:1987-1991: the reference abandons the root
+            if (l == 0) atomicAdd(&sp.ctr->depth_capped, 1u);
+            sz = 0;
+            break;
+        }
+        const uint32_t f = sz - 1;
+        const uint16_t tag = (uint16_t)(f + 1);
+        const uint32_t F = S.fr()[f];
+        const uint32_t res = fr_res(F), br = fr_br(F), st = fr_st(F);
+        if (st == 0) {
+            if (nc2 == 0) {   // leaf: emit (P, C1, X) (src:2005-2092)
+                const int nc1 = warp_sum(__popc(C1w));
+                bool ok = (int)np + nc1 >= q;
+                if (ok && np > 1) ok = ks_upper_bound(sp, R, S, np, Pw | C1w);
+                --sz;
+                if (ok) { emitted = 1; emitC = C1w; }
+                continue;
             }
-            ok = __shfl_sync(FULL, ok, 0);
-            if (!ok) return -1;
-            pos = __shfl_sync(FULL, pos, 0);
-            const unsigned long long slot = pos % pool->cap;
-            uint32_t* dst = sp.pool_data + slot * sp.slot_words;
-            write_task(sp, r, np, (uint32_t)nc, (uint32_t)nx, Pw, Cw, Xw, dst);
-            __threadfence();
-            __syncwarp();
-            if (l == 0) atomicExch(&sp.pool_seq[slot], (uint32_t)(pos + 1));
-            ++tasks;
-            return 1;
-        };
-
-        // bitset removal tagging for C1 against row M2[node] (updateCand13, src:1042-1097)
-        auto update13 = [&](uint32_t node, uint16_t tag) {
-            const uint32_t m2 = (l < W) ? __ldg(R.M2 + (uint64_t)node * W + l) : 0u;
-            uint32_t drop = C1w & ~m2;
-            C1w &= m2;
-            while (drop) { const int b = __ffs(drop) - 1; S.t1()[l * 32 + b] = tag; drop &= drop - 1; }
-        };
-        // order-preserving C2 filter (updateCand23, src:1099-1122)
-        auto update23 = [&](uint32_t node, uint16_t tag) {
-            const uint32_t* m2row = R.M2 + (uint64_t)node * W;
-            uint32_t write = 0;
-            for (uint32_t b = 0; b < nc2; b += 32) {
-                const uint32_t i = b + l;
-                uint16_t v = 0;
-                bool keep = false;
-                if (i < nc2) { v = S.c2()[i]; keep = (__ldg(m2row + (v >> 5)) >> (v & 31)) & 1u; }
-                const unsigned km = __ballot_sync(FULL, keep);
-                __syncwarp();
-                if (i < nc2) {
-                    if (keep) S.c2()[write + __popc(km & ((1u << l) - 1))] = v;
-                    else S.t2()[v] = tag;
-                }
-                write += __popc(km);
-                __syncwarp();
-            }
-            nc2 = write;
-        };
-        auto include = [&](uint32_t u) {
-            if (l == 0) S.P()[np] = u;
-            ++np;
-            if (l == (u >> 5)) Pw |= 1u << (u & 31);
-            __syncwarp();
-        };
-        auto x_add = [&](uint32_t u) { if (l == (u >> 5)) Xw |= 1u << (u & 31); };
-        auto x_del = [&](uint32_t u) { if (l == (u >> 5)) Xw &= ~(1u << (u & 31)); };
-        auto c2_pop = [&]() -> uint32_t { --nc2; return S.c2()[nc2]; };
-        auto c2_push = [&](uint32_t u) { if (l == 0) S.c2()[nc2] = (uint16_t)u; ++nc2; __syncwarp(); };
-        auto setfr = [&](uint32_t f, uint32_t val) { if (l == 0) S.fr()[f] = val; __syncwarp(); };
-
-        while (sz) {
-            if (sz >= (uint32_t)KS_MAX_DEPTH) {   // src:1987-1991: the reference abandons the root
-                if (l == 0) atomicAdd(&sp.ctr->depth_capped, 1u);
-                sz = 0;
-                break;
-            }
-            const uint32_t f = sz - 1;
-            const uint16_t tag = (uint16_t)(f + 1);
-            const uint32_t F = S.fr()[f];
-            const uint32_t res = fr_res(F), br = fr_br(F), st = fr_st(F);
-            __syncwarp();
-            if (st == 0) {
-                if (nc2 == 0) {
-                    const int nc1 = warp_sum(__popc(C1w));
-                    bool emitit = (int)np + nc1 >= q;
-                    if (emitit && np > 1) emitit = ks_upper_bound(sp, R, S, np, Pw | C1w, s_mask);
-                    --sz;
-                    if (emitit) {
-                        if (push_task(C1w) < 0) { if (l == 0) raise_error(sp.ctr, KPLEX_ERR_NOMEM); sz = 0; break; }
-                        if (pool_size_warp(sp) >= sp.pause_at) { paused = true; break; }
-                    }
-                    continue;
-                }
+            const uint32_t u = c2_pop();   // exclude the last C2 vertex first
+            if (l == (u >> 5)) Xw |= 1u << (u & 31);
+            setfr(f, fr_pack(res, br, 1, u));
+            setfr(sz, fr_pack(res, 1, 0, 0));
+            ++sz;
+            continue;
+        }
+        if (st == 1 || st == 3) {   // child returned: the excluded vertex goes back to C2's end
+            const uint32_t u = fr_v(F);
+            c2_push(u);
+            if (l == (u >> 5)) Xw &= ~(1u << (u & 31));
+            setfr(f, fr_pack(res, st == 3 ? br + 1 : br, 2, u));
+            continue;
+        }
+        if (st == 2) {
+            if (br < res) {   // include one more C2 vertex, exclude the next, recurse with res - br
                 const uint32_t u = c2_pop();
-                x_add(u);
-                setfr(f, fr_pack(res, br, 1, u));
-                setfr(sz, fr_pack(res, 1, 0, 0));
+                include(u);
+                update13(u, tag);
+                update23(u, tag);
+                if (nc2) {
+                    const uint32_t w = c2_pop();
+                    if (l == (w >> 5)) Xw |= 1u << (w & 31);
+                    setfr(f, fr_pack(res, br, 3, w));
+                } else {
+                    setfr(f, fr_pack(res, br, 4, 0));
+                }
+                setfr(sz, fr_pack(res - br, 1, 0, 0));
                 ++sz;
                 continue;
             }
-            if (st == 1 || st == 3) {
-                const uint32_t u = fr_v(F);
-                c2_push(u);
-                x_del(u);
-                setfr(f, fr_pack(res, st == 3 ? br + 1 : br, 2, u));
-                continue;
-            }
-            if (st == 2) {
-                if (br < res) {
-                    const uint32_t u = c2_pop();
-                    include(u);
-                    update13(u, tag);
-                    update23(u, tag);
-                    if (nc2) {
-                        const uint32_t w = c2_pop();
-                        x_add(w);
-                        setfr(f, fr_pack(res, br, 3, w));
-                    } else {
-                        setfr(f, fr_pack(res, br, 4, 0));
-                    }
-                    setfr(sz, fr_pack(res - br, 1, 0, 0));
-                    ++sz;
-                    continue;
-                }
-                setfr(f, fr_pack(res, br, 4, 0));
-                continue;
-            }
-            if (st == 4) {
-                if (br == res) {
-                    const uint32_t u = c2_pop();
-                    include(u);
-                    update13(u, tag);
-                    setfr(f, fr_pack(res, br, 5, 0));
-                    const int nc1 = warp_sum(__popc(C1w));
-                    if ((int)np + nc1 < q) continue;
-                    if (np > 1 && !ks_upper_bound(sp, R, S, np, Pw | C1w, s_mask)) continue;
-                    // isKplex2 filter of C1 (src:2296-2313): c stays if P+c is a k-plex
-                    s_mask[l] = Pw;
-                    __syncwarp();
-                    // saturated P members: neiInP + k == |P|
-                    s_aux[l] = 0u;
-                    __syncwarp();
-                    for (uint32_t i = l; i < np; i += 32) {
-                        const uint32_t v = S.P()[i];
-                        const int pv = row_and_popc(R.A + (uint64_t)v * W, s_mask, W);
-                        if (pv + k == (int)np) atomicOr(&s_aux[v >> 5], 1u << (v & 31));
-                    }
-                    __syncwarp();
-                    uint32_t keepw = 0;
-                    {
-                        // every C1 bit of this lane's word, checked by this lane
-                        uint32_t c = C1w;
-                        while (c) {
-                            const int b = __ffs(c) - 1;
-                            c &= c - 1;
-                            const uint32_t v = l * 32 + b;
-                            const uint32_t* row = R.A + (uint64_t)v * W;
-                            const int pv = row_and_popc(row, s_mask, W);
-                            bool ok = pv + k >= (int)np + 1;
-                            for (uint32_t w = 0; ok && w < W; ++w) if (s_aux[w] & ~__ldg(row + w)) ok = false;
-                            if (ok) keepw |= 1u << b;
-                        }
-                    }
-                    if (push_task(keepw) < 0) { if (l == 0) raise_error(sp.ctr, KPLEX_ERR_NOMEM); sz = 0; break; }
-                    if (pool_size_warp(sp) >= sp.pause_at) { paused = true; break; }
-                    continue;
-                }
-                setfr(f, fr_pack(res, br, 5, 0));
-                continue;
-            }
-            // st == 5: undo this frame (src:2405-2441)
-            for (uint32_t i = 0; i < br; ++i) {
-                const uint32_t node = S.P()[np - 1];
-                --np;
-                if (l == (node >> 5)) Pw &= ~(1u << (node & 31));
-                c2_push(node);
-            }
-            for (uint32_t b = 0; b < n; b += 32) {
-                const uint32_t i = b + l;
-                bool h1 = false, h2 = false;
-                if (i < n) { h1 = S.t1()[i] == tag; h2 = S.t2()[i] == tag; }
-                const unsigned m1 = __ballot_sync(FULL, h1), m2 = __ballot_sync(FULL, h2);
-                if (h1) S.t1()[i] = 0;
-                if (h2) { S.t2()[i] = 0; S.c2()[nc2 + __popc(m2 & ((1u << l) - 1))] = (uint16_t)i; }
-                if (l == (b >> 5)) C1w |= m1;
-                nc2 += __popc(m2);
+            setfr(f, fr_pack(res, br, 4, 0));
+            continue;
+        }
+        if (st == 4) {
+            setfr(f, fr_pack(res, br, 5, 0));
+            if (br == res) {   // budget used: include the last one and emit with C1 filtered (src:2259-2403)
+                const uint32_t u = c2_pop();
+                include(u);
+                update13(u, tag);
+                const int nc1 = warp_sum(__popc(C1w));
+                if ((int)np + nc1 < q) continue;
+                if (np > 1 && !ks_upper_bound(sp, R, S, np, Pw | C1w)) continue;
+                // isKplex2 (src:568-584): c stays if P + c is a k-plex
+                S.mask()[l] = Pw;
+                S.aux()[l] = 0u;
+                S.keep()[l] = 0u;
                 __syncwarp();
+                for (uint32_t i = l; i < np; i += 32) {
+                    const uint32_t v = S.P()[i];
+                    if (row_and_popc(R.A + (uint64_t)v * W, S.mask(), W) + k == (int)np) atomicOr(&S.aux()[v >> 5], 1u << (v & 31));
+                }
+                const int m1 = bits_to_list(C1w, S.lst());
+                for (int i = l; i < m1; i += 32) {
+                    const uint32_t v = S.lst()[i];
+                    const uint32_t* row = R.A + (uint64_t)v * W;
+                    bool ok = row_and_popc(row, S.mask(), W) + k >= (int)np + 1;
+                    for (uint32_t w = 0; ok && w < W; ++w) if (S.aux()[w] & ~__ldg(row + w)) ok = false;
+                    if (ok) atomicOr(&S.keep()[v >> 5], 1u << (v & 31));
+                }
+                __syncwarp();
+                emitted = 1;
+                emitC = S.keep()[l];
+                continue;
             }
-            --sz;
+            continue;
         }
-        // save or finish
-        S.bits()[l] = C1w; S.bits()[MAX_WORDS + l] = Xw; S.bits()[2 * MAX_WORDS + l] = Pw;
-        if (l == 0) { S.sz() = sz; S.np() = np; S.nc2() = nc2; if (!paused || sz == 0) S.root() = (sz == 0) ? 0xffffffffu : r; }
-        __syncwarp();
-        if (paused) {
-            if (l == 0) { if (sz == 0) S.root() = 0xffffffffu; atomicAdd(&sp.ctr->ks_paused, 1u); }
-            break;
+        // st == 5: undo this frame (src:2405-2441)
+        for (uint32_t i = 0; i < br; ++i) {
+            const uint32_t node = S.P()[np - 1];
+            --np;
+            if (l == (node >> 5)) Pw &= ~(1u << (node & 31));
+            c2_push(node);
         }
+        for (uint32_t b = 0; b < n; b += 32) {
+            const uint32_t i = b + l;
+            bool h1 = false, h2 = false;
+            if (i < n) { h1 = S.t1()[i] == tag; h2 = S.t2()[i] == tag; }
+            const unsigned m1 = __ballot_sync(FULL, h1), m2 = __ballot_sync(FULL, h2);
+            if (h1) S.t1()[i] = 0;
+            if (h2) { S.t2()[i] = 0; S.c2()[nc2 + __popc(m2 & ((1u << l) - 1))] = (uint16_t)i; }
+            if (l == (b >> 5)) C1w |= m1;
+            nc2 += __popc(m2);
+            __syncwarp();
+        }
+        --sz;
     }
-    if (l == 0 && tasks) atomicAdd(&sp.ctr->tasks, tasks);
+    if (emitted) {
+        e->np = np;
+        e->nc = (uint32_t)warp_sum(__popc(emitC));
+        e->nx = (uint32_t)warp_sum(__popc(Xw));
+        e->Pw = Pw; e->Cw = emitC; e->Xw = Xw;
+    }
+    __syncwarp();
+    S.bits()[l] = C1w;
+    S.bits()[MAX_WORDS + l] = Xw;
+    S.bits()[2 * MAX_WORDS + l] = Pw;
+    if (l == 0) { S.sz() = sz; S.np() = np; S.nc2() = nc2; }
+    __syncwarp();
+    return emitted;
 }
-
 
 // ============================================================== branch-and-bound
 struct BnbSmem {
-    uint32_t* rec;    // slot_words: record being loaded
+    uint32_t* rec;    // slot_words: record being loaded from the pool
     uint32_t* P;      // 32 words each
     uint32_t* PC;
     uint32_t* SAT;
@@ -397,9 +350,9 @@ __device__ inline BnbSmem bnb_smem(uint32_t* base, uint32_t nmax, uint32_t slot_
     return m;
 }
 
-// The reference's warp pivot rule (src:1628-1663, 1669-1697): combine keeps
-// the current pivot unless the other lane's is strictly smaller in neiInG or
-// equal with a strictly smaller neiInP.
+// The reference's warp pivot rule (src:1628-1663, 1669-1697): the shfl_down
+// tree keeps the current pivot unless the other lane's is strictly smaller in
+// neiInG, or equal with a strictly smaller neiInP.
 __device__ __forceinline__ void pivot_tree(int& m, int& v, int& p, int& idx) {
 #pragma unroll
     for (int o = 16; o; o >>= 1) {
@@ -415,8 +368,8 @@ __device__ __forceinline__ void pivot_tree(int& m, int& v, int& p, int& idx) {
 
 // isMaximal_opt / isMaximalPC_opt (src:703-1000): true when no vertex of the
 // root's left set extends S (list[0..s), degrees deg[], bitset sS) to a k-plex.
-// Candidates must be adjacent to every saturated member of S and to one of
-// any k members; each candidate's count is its popcount against S.
+// Candidates must be adjacent to every saturated member of S and to one of any
+// k members; each candidate's count is its popcount against S.
 __device__ bool left_maximal(const SearchParams& sp, const RootView& R, const BnbSmem& m, int s, const uint16_t* deg,
                              const uint32_t* sS, unsigned long long& bb) {
     const unsigned l = lane_id();
@@ -447,17 +400,17 @@ __device__ bool left_maximal(const SearchParams& sp, const RootView& R, const Bn
     lc &= un;
     bool found = false;
     uint32_t c = lc;
-    int nbb = 0;
+    int nrows = 0;
     while (c && !found) {
         const int b = __ffs(c) - 1;
         c &= c - 1;
         const uint32_t j = l * 32 + b;
         const int cnt = row_and_popc(R.LT + (uint64_t)j * W, sS, W);
-        ++nbb;
+        ++nrows;
         if (cnt + k >= s + 1) found = true;
     }
-    nbb = warp_sum(nbb);
-    if (l == 0) bb += (unsigned long long)nbb * 4ull * W + (unsigned long long)(k + 1) * 4ull * WL;
+    nrows = warp_sum(nrows);
+    if (l == 0) bb += (unsigned long long)nrows * 4ull * W + (unsigned long long)(k + 1) * 4ull * WL;
     return !__any_sync(FULL, found);
 }
 
@@ -489,29 +442,316 @@ __device__ void emit_plex(const SearchParams& sp, const RootView& R, const BnbSm
     if (l == 0) hsum += x;
 }
 
-__global__ void __launch_bounds__(256) bnb_kernel(SearchParams sp, uint32_t nmax) {
+struct Node {
+    uint32_t root, np, nc, nx;
+    uint32_t Pw, Cw, Xw;   // this lane's word of each bitset
+};
+
+struct WarpWork {
+    uint32_t* stack;
+    unsigned long long sbot, stop;
+    unsigned long long cnt, hsum, tasks, nodes, bb;
+};
+
+// One branch-and-bound node (BNB, src:1516-1724).  Returns true when the node
+// produced an include child, which is left in *t; the exclude child is pushed
+// on the warp's stack.
+__device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootView& R, Node* t, WarpWork& ww) {
+    const unsigned l = lane_id();
+    const int k = sp.k, q = sp.q;
+    const uint32_t W = R.W, Wt = sp.Wt, SW = sp.slot_words;
+    const uint32_t np = t->np, nc = t->nc, nx = t->nx;
+    const uint32_t Pw = t->Pw, Cw = t->Cw, Xw = t->Xw;
+    if ((int)(np + nc) < q) return false;
+    m.P[l] = Pw;
+    m.PC[l] = Pw | Cw;
+    __syncwarp();
+    bits_to_list(Pw, m.list);
+    bits_to_list(Cw, m.list + np);
+    const int tot = (int)(np + nc);
+    for (int i = l; i < tot; i += 32) {
+        const uint32_t* row = R.A + (uint64_t)m.list[i] * W;
+        m.gv[i] = (uint16_t)row_and_popc(row, m.PC, W);
+        m.pv[i] = (uint16_t)row_and_popc(row, m.P, W);
+    }
+    if (l == 0) ww.bb += (unsigned long long)(tot + 3) * 4ull * W;   // rows + the record's P, C, X
+    __syncwarp();
+    if (nc == 0) {   // src:1579-1588
+        if (nx == 0 && (int)np >= q && left_maximal(sp, R, m, (int)np, m.pv, m.P, ww.bb))
+            emit_plex(sp, R, m, (int)np, ww.cnt, ww.hsum);
+        return false;
+    }
+    // pivot in P: minimum neiInG, ties to the smaller index (src:1592-1620)
+    unsigned long long key = ~0ull;
+    for (int i = l; i < (int)np; i += 32) {
+        const unsigned long long kk = ((unsigned long long)m.gv[i] << 32) | ((unsigned long long)m.list[i] << 16) | m.pv[i];
+        key = kk < key ? kk : key;
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) { const unsigned long long ok = __shfl_xor_sync(FULL, key, o); key = ok < key ? ok : key; }
+    const int minP = (int)(key >> 32);
+    const int pp = (int)((key >> 16) & 0xffff);
+    const int ppP = (int)(key & 0xffff);
+    if (minP + k < max(q, (int)np)) return false;   // src:1624
+    int piv, pmin, pval, pidx;
+    if (minP + k < tot) {
+        // candidates not adjacent to the P pivot (src:1626-1663)
+        m.ROW[l] = (l < W) ? __ldg(R.A + (uint64_t)pp * W + l) : 0u;
+        __syncwarp();
+        pmin = INT_MAX; piv = -1; pval = 0; pidx = -1;
+        for (int i = l; i < (int)nc; i += 32) {
+            const uint32_t v = m.list[np + i];
+            if (test_bit(m.ROW, v)) continue;
+            const int g = m.gv[np + i], p = m.pv[np + i];
+            if (g < pmin) { pmin = g; piv = (int)v; pval = p; pidx = (int)np + i; }
+            else if (g == pmin && pval > p) { piv = (int)v; pval = p; pidx = (int)np + i; }
+        }
+        pivot_tree(pmin, piv, pval, pidx);
+    } else {
+        // minimum over P (seeded) and C (src:1669-1697)
+        pmin = minP; piv = pp; pval = ppP; pidx = -2;
+        for (int i = l; i < (int)nc; i += 32) {
+            const uint32_t v = m.list[np + i];
+            const int g = m.gv[np + i], p = m.pv[np + i];
+            if (g < pmin) { pmin = g; piv = (int)v; pval = p; pidx = (int)np + i; }
+            else if (g == pmin && pval > p) { piv = (int)v; pval = p; pidx = (int)np + i; }
+        }
+        pivot_tree(pmin, piv, pval, pidx);
+        if (pmin >= tot - k) {
+            // P ∪ C is a k-plex (src:1698-1717)
+            if (tot < q) return false;
+            const int nxl = bits_to_list(Xw, m.list + tot);
+            for (int i = l; i < nxl; i += 32)
+                m.gv[tot + i] = (uint16_t)row_and_popc(R.A + (uint64_t)m.list[tot + i] * W, m.PC, W);
+            m.SAT[l] = 0u;
+            __syncwarp();
+            for (int i = l; i < tot; i += 32)
+                if ((int)m.gv[i] + k == tot) { const uint32_t u = m.list[i]; atomicOr(&m.SAT[u >> 5], 1u << (u & 31)); }
+            __syncwarp();
+            bool ext = false;
+            for (int i = l; i < nxl; i += 32) {   // isKplexPC2 src:601-622
+                if ((int)m.gv[tot + i] + k < tot + 1) continue;
+                const uint32_t* row = R.A + (uint64_t)m.list[tot + i] * W;
+                bool ok = true;
+                for (uint32_t w = 0; ok && w < W; ++w) if (m.SAT[w] & ~__ldg(row + w)) ok = false;
+                ext |= ok;
+            }
+            if (l == 0) ww.bb += (unsigned long long)nxl * 4ull * W;
+            if (__any_sync(FULL, ext)) return false;
+            if (left_maximal(sp, R, m, tot, m.gv, m.PC, ww.bb)) emit_plex(sp, R, m, tot, ww.cnt, ww.hsum);
+            return false;
+        }
+    }
+    // ---------------- branch on piv (src:1197-1465)
+    if (piv < 0 || pidx < 0) { if (l == 0) raise_error(sp.ctr, KPLEX_ERR_INTERNAL); return false; }
+    const uint32_t v = (uint32_t)piv;
+    const uint32_t vw = v >> 5, vb = 1u << (v & 31);
+    {   // exclude child -> this warp's stack
+        if (ww.stop - ww.sbot >= sp.stack_depth) { if (l == 0) raise_error(sp.ctr, KPLEX_ERR_INTERNAL); return false; }
+        uint32_t* dst = ww.stack + (ww.stop % sp.stack_depth) * SW;
+        const uint32_t Cx = (l == vw) ? (Cw & ~vb) : Cw;
+        const uint32_t Xx = (l == vw) ? (Xw | vb) : Xw;
+        if (l == 0) { __stcg(dst + 0, t->root); __stcg(dst + 1, np | ((nc - 1) << 16)); __stcg(dst + 2, nx + 1); __stcg(dst + 3, 0u); }
+        if (l < Wt) { __stcg(dst + 4 + l, Pw); __stcg(dst + 4 + Wt + l, Cx); __stcg(dst + 4 + 2 * Wt + l, Xx); }
+        ++ww.stop;
+        if (l == 0) { ++ww.tasks; ww.bb += 12ull * W; }
+    }
+    // include child
+    const uint32_t np1 = np + 1;
+    const uint32_t P1 = (l == vw) ? (Pw | vb) : Pw;
+    m.ROW[l] = (l < W) ? __ldg(R.A + (uint64_t)v * W + l) : 0u;
+    m.M2[l] = (l < W) ? __ldg(R.M2 + (uint64_t)v * W + l) : 0u;
+    m.M4[l] = (l < W) ? __ldg(R.M4 + (uint64_t)v * W + l) : 0u;
+    m.SAT[l] = 0u;
+    m.NC[l] = 0u;
+    m.NX[l] = 0u;
+    __syncwarp();
+    // saturated members of P + v: neiInP' + k == |P'|
+    for (int i = l; i < (int)np; i += 32) {
+        const uint32_t u = m.list[i];
+        const int pu = (int)m.pv[i] + (int)test_bit(m.ROW, u);
+        if (pu + k == (int)np1) atomicOr(&m.SAT[u >> 5], 1u << (u & 31));
+    }
+    if (l == 0 && (int)m.pv[pidx] + k == (int)np1) atomicOr(&m.SAT[vw], vb);
+    m.P[l] = P1;
+    __syncwarp();
+    // C filter: class >= UNLINK2EQUAL and P' + c a k-plex (isKplex3)
+    for (int i = l; i < (int)nc; i += 32) {
+        const uint32_t c = m.list[np + i];
+        if (c == v || !test_bit(m.M2, c)) continue;
+        const uint32_t* row = R.A + (uint64_t)c * W;
+        const int pc = (int)m.pv[np + i] + (int)test_bit(m.ROW, c);
+        if (pc + k < (int)np1 + 1) continue;
+        bool ok = true;
+        for (uint32_t w = 0; ok && w < W; ++w) if (m.SAT[w] & ~__ldg(row + w)) ok = false;
+        if (ok) atomicOr(&m.NC[c >> 5], 1u << (c & 31));
+    }
+    if (l == 0) ww.bb += (unsigned long long)nc * 4ull * W;
+    __syncwarp();
+    const uint32_t C1 = m.NC[l];
+    const uint32_t nc1 = (uint32_t)warp_sum(__popc(C1));
+    m.PC[l] = P1 | C1;
+    __syncwarp();
+    // upperBound2 over P' (src:1022-1040)
+    bool ub = true;
+    for (int i = l; i <= (int)np; i += 32) {
+        const uint32_t u = (i < (int)np) ? m.list[i] : v;
+        if (row_and_popc(R.A + (uint64_t)u * W, m.PC, W) + k < q) ub = false;
+    }
+    if (l == 0) ww.bb += (unsigned long long)np1 * 4ull * W;
+    if (!__all_sync(FULL, ub)) return false;
+    // X filter: class >= UNLINK2MORE and P' + x a k-plex
+    const int nxl = bits_to_list(Xw, m.list);
+    for (int i = l; i < nxl; i += 32) {
+        const uint32_t x = m.list[i];
+        if (!test_bit(m.M4, x)) continue;
+        const uint32_t* row = R.A + (uint64_t)x * W;
+        if (row_and_popc(row, m.P, W) + k < (int)np1 + 1) continue;
+        bool ok = true;
+        for (uint32_t w = 0; ok && w < W; ++w) if (m.SAT[w] & ~__ldg(row + w)) ok = false;
+        if (ok) atomicOr(&m.NX[x >> 5], 1u << (x & 31));
+    }
+    if (l == 0) ww.bb += (unsigned long long)nxl * 4ull * W;
+    __syncwarp();
+    const uint32_t X1 = m.NX[l];
+    t->nx = (uint32_t)warp_sum(__popc(X1));
+    t->Pw = P1; t->Cw = C1; t->Xw = X1;
+    t->np = np1; t->nc = nc1;
+    if (l == 0) { ++ww.tasks; ww.bb += 12ull * W; }
+    return true;
+}
+
+// ============================================================== the persistent kernel
+__device__ __forceinline__ void load_record(const uint32_t* src, uint32_t Wt, Node* t, bool cg) {
+    const unsigned l = lane_id();
+    if (cg) {
+        t->root = __ldcg(src);
+        const uint32_t h1 = __ldcg(src + 1);
+        t->np = h1 & 0xffff; t->nc = h1 >> 16; t->nx = __ldcg(src + 2);
+        t->Pw = (l < Wt) ? __ldcg(src + 4 + l) : 0u;
+        t->Cw = (l < Wt) ? __ldcg(src + 4 + Wt + l) : 0u;
+        t->Xw = (l < Wt) ? __ldcg(src + 4 + 2 * Wt + l) : 0u;
+    } else {
+        t->root = src[0];
+        t->np = src[1] & 0xffff; t->nc = src[1] >> 16; t->nx = src[2];
+        t->Pw = (l < Wt) ? src[4 + l] : 0u;
+        t->Cw = (l < Wt) ? src[4 + Wt + l] : 0u;
+        t->Xw = (l < Wt) ? src[4 + 2 * Wt + l] : 0u;
+    }
+}
+
+__global__ void __launch_bounds__(256, 3) search_kernel(SearchParams sp, uint32_t nmax) {
     extern __shared__ uint4 smem4[];
     uint32_t* smem = reinterpret_cast<uint32_t*>(smem4);
     const unsigned l = lane_id();
     const unsigned wib = threadIdx.x >> 5;
     const unsigned warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t SW = sp.slot_words, Wt = sp.Wt;
-    const BnbSmem m = bnb_smem(smem + wib * bnb_smem_words(nmax, SW), nmax, SW);
-    uint32_t* stack = sp.stacks + (uint64_t)warp * sp.stack_depth * SW;
-    const int k = sp.k, q = sp.q;
-
-    unsigned long long cnt = 0, hsum = 0, tasks = 0, nodes = 0, bb = 0;   // nodes: warp-uniform
-    unsigned long long sbot = 0, stop = 0;
+    const bool producer = (wib == 0);
+    const KsSlot S{smem};
+    const BnbSmem m = bnb_smem(smem + KS_WORDS + wib * bnb_smem_words(nmax, SW), nmax, SW);
+    WarpWork ww;
+    ww.stack = sp.stacks + (uint64_t)warp * sp.stack_depth * SW;
+    ww.sbot = ww.stop = 0;
+    ww.cnt = ww.hsum = ww.tasks = ww.nodes = ww.bb = 0;
+    unsigned long long ks_tasks = 0;
+    const unsigned long long resume_at = sp.pause_at / 2 > 0 ? sp.pause_at / 2 : 1;
+    bool have = false, counted = false, ks_active = false, paused = false;
     unsigned long long idle = 0;
+    Node t{};
     uint32_t cur_root = 0xffffffffu;
     RootView R{};
+    Emitted e{};
 
     for (;;) {
-        // ---------------- acquire a record from the pool
-        // A warp counts itself busy only while it may hold a record, and idle
-        // warps touch the counter only when the pool is non-empty, so the exit
-        // test (pool empty and nobody busy) cannot be held off by idle warps.
-        int got = 0;
+        // ---------------- local depth-first work
+        if (!have && ww.stop > ww.sbot) {
+            --ww.stop;
+            load_record(ww.stack + (ww.stop % sp.stack_depth) * SW, Wt, &t, true);
+            have = true;
+            __syncwarp();
+        }
+        if (have) {
+            if (ww.stop - ww.sbot >= 2 && (ww.nodes & 7) == 0) {   // donate the oldest stacked record
+                int give = 0;
+                if (l == 0) give = pool_size(sp) < sp.low_water;
+                give = __shfl_sync(FULL, give, 0);
+                if (give) {
+                    const uint32_t* src = ww.stack + (ww.sbot % sp.stack_depth) * SW;
+                    if (pool_push(sp, [&](unsigned i) { return __ldcg(src + i); })) ++ww.sbot;
+                }
+            }
+            if (t.root != cur_root) { R = root_view(sp, t.root); cur_root = t.root; }
+            ++ww.nodes;
+            have = bnb_node(sp, m, R, &t, ww);
+            __syncwarp();
+            if (!have && ww.stop == ww.sbot) {
+                ww.stop = ww.sbot = 0;
+                if (counted) { if (l == 0) atomicSub(&sp.ctr->busy, 1u); counted = false; }
+            }
+            continue;
+        }
+        // ---------------- producer: k-search
+        if (producer) {
+            const unsigned long long ps = pool_size_warp(sp);
+            if (paused && ps < resume_at) paused = false;
+            if (!paused && ps >= sp.pause_at) {
+                paused = true;
+                if (l == 0) atomicAdd(&sp.ctr->ks_paused, 1u);
+            }
+            if (!paused) {
+                if (!ks_active) {
+                    // claim the next valid root; ks_active rises before the claim so that
+                    // consumers never see "all roots claimed" with a claim in flight
+                    for (;;) {
+                        int r = -1;
+                        if (l == 0 && *(volatile unsigned*)&sp.ctr->next_root < sp.nroots) {
+                            atomicAdd(&sp.ctr->ks_active, 1u);
+                            const unsigned c = atomicAdd(&sp.ctr->next_root, 1u);
+                            if (c < sp.nroots) r = (int)c;
+                            else atomicSub(&sp.ctr->ks_active, 1u);
+                        }
+                        r = __shfl_sync(FULL, r, 0);
+                        if (r < 0) break;
+                        const RootDesc d = sp.roots[r];
+                        if ((d.flags & ROOT_VALID) && d.n) { ks_start(sp, S, (uint32_t)r, d); ks_active = true; break; }
+                        if (l == 0) atomicSub(&sp.ctr->ks_active, 1u);
+                    }
+                }
+                if (ks_active) {
+                    const int got = ks_advance(sp, S, &e);
+                    if (got) {
+                        ++ks_tasks;
+                        const uint32_t r = S.root();
+                        // stage this lane's words in shared memory; the record is hdr | P | C | X
+                        m.P[l] = e.Pw; m.NC[l] = e.Cw; m.NX[l] = e.Xw;
+                        __syncwarp();
+                        const bool pushed = pool_push(sp, [&](unsigned i) -> uint32_t {
+                            if (i == 0) return r;
+                            if (i == 1) return e.np | (e.nc << 16);
+                            if (i == 2) return e.nx;
+                            if (i < 4) return 0u;
+                            const unsigned j = i - 4, which = j / Wt, wi = j % Wt;
+                            return which == 0 ? m.P[wi] : (which == 1 ? m.NC[wi] : m.NX[wi]);
+                        });
+                        if (!pushed) {   // ring full: keep the task
+                            t.root = r; t.np = e.np; t.nc = e.nc; t.nx = e.nx;
+                            t.Pw = e.Pw; t.Cw = e.Cw; t.Xw = e.Xw;
+                            have = true;
+                            if (!counted) { if (l == 0) atomicAdd(&sp.ctr->busy, 1u); counted = true; }
+                        }
+                    } else {
+                        ks_active = false;
+                        __syncwarp();
+                        if (l == 0) { S.root() = 0xffffffffu; __threadfence(); atomicSub(&sp.ctr->ks_active, 1u); }
+                        __syncwarp();
+                    }
+                    idle = 0;
+                    continue;
+                }
+            }
+        }
+        // ---------------- consumer: take a record from the pool
         {
             int nonempty = 0;
             if (l == 0) nonempty = pool_size(sp) > 0;
@@ -519,234 +759,45 @@ __global__ void __launch_bounds__(256) bnb_kernel(SearchParams sp, uint32_t nmax
             if (nonempty) {
                 if (l == 0) atomicAdd(&sp.ctr->busy, 1u);
                 __syncwarp();
-                got = pool_pop(sp, m.rec) ? 1 : 0;
-                if (!got && l == 0) atomicSub(&sp.ctr->busy, 1u);
-            }
-        }
-        if (!got) {
-            int done = 0;
-            if (l == 0) {
-                __threadfence();
-                const unsigned long long ps = pool_size(sp);
-                const unsigned b = *(volatile unsigned*)&sp.ctr->busy;
-                done = (ps == 0 && b == 0);
-            }
-            done = __shfl_sync(FULL, done, 0);
-            if (done) break;
-            if (++idle > sp.spin_limit) {
-                if (l == 0) atomicAdd(&sp.ctr->timeouts, 1u);
-                break;
-            }
-            __nanosleep(idle < 64 ? 100 : 2000);
-            continue;
-        }
-        idle = 0;
-        __syncwarp();
-        // registers: header + this lane's words of P, C, X
-        uint32_t root = m.rec[0];
-        uint32_t np = m.rec[1] & 0xffff, nc = m.rec[1] >> 16, nx = m.rec[2];
-        uint32_t Pw = (l < Wt) ? m.rec[4 + l] : 0u;
-        uint32_t Cw = (l < Wt) ? m.rec[4 + Wt + l] : 0u;
-        uint32_t Xw = (l < Wt) ? m.rec[4 + 2 * Wt + l] : 0u;
-        __syncwarp();
-
-        for (;;) {   // ---------------- depth-first over this warp's records
-            // donate the oldest stacked record when the pool runs low
-            if (stop - sbot >= 2 && (nodes & 7) == 0) {
-                int give = 0;
-                if (l == 0) give = pool_size(sp) < sp.low_water;
-                give = __shfl_sync(FULL, give, 0);
-                if (give) {
-                    const uint32_t* src = stack + (sbot % sp.stack_depth) * SW;
-                    if (pool_push(sp, [&](unsigned i) { return __ldcg(src + i); })) ++sbot;
-                }
-            }
-            if (root != cur_root) { R = root_view(sp, root); cur_root = root; }
-            const uint32_t W = R.W;
-            ++nodes;
-            bool have_child = false;
-            do {
-                if ((int)(np + nc) < q) break;
-                m.P[l] = Pw;
-                m.PC[l] = Pw | Cw;
-                __syncwarp();
-                bits_to_list(Pw, m.list);
-                bits_to_list(Cw, m.list + np);
-                const int tot = (int)(np + nc);
-                for (int i = l; i < tot; i += 32) {
-                    const uint32_t* row = R.A + (uint64_t)m.list[i] * W;
-                    m.gv[i] = (uint16_t)row_and_popc(row, m.PC, W);
-                    m.pv[i] = (uint16_t)row_and_popc(row, m.P, W);
-                }
-                if (l == 0) bb += (unsigned long long)(tot + 3) * 4ull * W;   // rows + the record's P, C, X
-                __syncwarp();
-                if (nc == 0) {   // src:1579-1588
-                    if (nx == 0 && (int)np >= q && left_maximal(sp, R, m, (int)np, m.pv, m.P, bb))
-                        emit_plex(sp, R, m, (int)np, cnt, hsum);
-                    break;
-                }
-                // pivot in P: minimum neiInG, ties to the smaller index (src:1592-1620)
-                unsigned long long key = ~0ull;
-                for (int i = l; i < (int)np; i += 32) {
-                    const unsigned long long kk = ((unsigned long long)m.gv[i] << 32) | ((unsigned long long)m.list[i] << 16) | m.pv[i];
-                    key = kk < key ? kk : key;
-                }
-#pragma unroll
-                for (int o = 16; o; o >>= 1) { const unsigned long long ok = __shfl_xor_sync(FULL, key, o); key = ok < key ? ok : key; }
-                const int minP = (int)(key >> 32);
-                const int pp = (int)((key >> 16) & 0xffff);
-                const int ppP = (int)(key & 0xffff);
-                if (minP + k < max(q, (int)np)) break;   // src:1624
-                int piv, pmin, pval, pidx;
-                if (minP + k < tot) {
-                    // candidates not adjacent to the P pivot (src:1626-1663)
-                    m.ROW[l] = (l < W) ? __ldg(R.A + (uint64_t)pp * W + l) : 0u;
+                if (pool_pop(sp, m.rec)) {
+                    load_record(m.rec, Wt, &t, false);
+                    have = true;
+                    counted = true;
+                    idle = 0;
                     __syncwarp();
-                    pmin = INT_MAX; piv = -1; pval = 0; pidx = -1;
-                    for (int i = l; i < (int)nc; i += 32) {
-                        const uint32_t v = m.list[np + i];
-                        if (test_bit(m.ROW, v)) continue;
-                        const int g = m.gv[np + i], p = m.pv[np + i];
-                        if (g < pmin) { pmin = g; piv = (int)v; pval = p; pidx = (int)np + i; }
-                        else if (g == pmin && pval > p) { piv = (int)v; pval = p; pidx = (int)np + i; }
-                    }
-                    pivot_tree(pmin, piv, pval, pidx);
-                } else {
-                    // minimum over P (seeded) and C (src:1669-1697)
-                    pmin = minP; piv = pp; pval = ppP; pidx = -2;
-                    for (int i = l; i < (int)nc; i += 32) {
-                        const uint32_t v = m.list[np + i];
-                        const int g = m.gv[np + i], p = m.pv[np + i];
-                        if (g < pmin) { pmin = g; piv = (int)v; pval = p; pidx = (int)np + i; }
-                        else if (g == pmin && pval > p) { piv = (int)v; pval = p; pidx = (int)np + i; }
-                    }
-                    pivot_tree(pmin, piv, pval, pidx);
-                    if (pmin >= tot - k) {
-                        // P ∪ C is a k-plex (src:1698-1717)
-                        if (tot < q) break;
-                        const int nxl = bits_to_list(Xw, m.list + tot);
-                        for (int i = l; i < nxl; i += 32)
-                            m.gv[tot + i] = (uint16_t)row_and_popc(R.A + (uint64_t)m.list[tot + i] * W, m.PC, W);
-                        m.SAT[l] = 0u;
-                        __syncwarp();
-                        for (int i = l; i < tot; i += 32)
-                            if ((int)m.gv[i] + k == tot) { const uint32_t u = m.list[i]; atomicOr(&m.SAT[u >> 5], 1u << (u & 31)); }
-                        __syncwarp();
-                        bool ext = false;
-                        for (int i = l; i < nxl; i += 32) {   // isKplexPC2 src:601-622
-                            if ((int)m.gv[tot + i] + k < tot + 1) continue;
-                            const uint32_t* row = R.A + (uint64_t)m.list[tot + i] * W;
-                            bool ok = true;
-                            for (uint32_t w = 0; ok && w < W; ++w) if (m.SAT[w] & ~__ldg(row + w)) ok = false;
-                            ext |= ok;
-                        }
-                        if (l == 0) bb += (unsigned long long)nxl * 4ull * W;
-                        if (__any_sync(FULL, ext)) break;
-                        if (left_maximal(sp, R, m, tot, m.gv, m.PC, bb)) emit_plex(sp, R, m, tot, cnt, hsum);
-                        break;
-                    }
+                    continue;
                 }
-                // ---------------- branch on piv (src:1197-1465)
-                if (piv < 0 || pidx < 0) { if (l == 0) raise_error(sp.ctr, KPLEX_ERR_INTERNAL); break; }
-                const uint32_t v = (uint32_t)piv;
-                const uint32_t vw = v >> 5, vb = 1u << (v & 31);
-                {   // exclude child -> this warp's stack
-                    if (stop - sbot >= sp.stack_depth) { if (l == 0) raise_error(sp.ctr, KPLEX_ERR_INTERNAL); break; }
-                    uint32_t* dst = stack + (stop % sp.stack_depth) * SW;
-                    const uint32_t Cx = (l == vw) ? (Cw & ~vb) : Cw;
-                    const uint32_t Xx = (l == vw) ? (Xw | vb) : Xw;
-                    if (l == 0) { __stcg(dst + 0, root); __stcg(dst + 1, np | ((nc - 1) << 16)); __stcg(dst + 2, nx + 1); __stcg(dst + 3, 0u); }
-                    if (l < Wt) { __stcg(dst + 4 + l, Pw); __stcg(dst + 4 + Wt + l, Cx); __stcg(dst + 4 + 2 * Wt + l, Xx); }
-                    ++stop;
-                    if (l == 0) { ++tasks; bb += 12ull * W; }
-                }
-                // include child
-                const uint32_t np1 = np + 1;
-                const uint32_t P1 = (l == vw) ? (Pw | vb) : Pw;
-                m.ROW[l] = (l < W) ? __ldg(R.A + (uint64_t)v * W + l) : 0u;
-                m.M2[l] = (l < W) ? __ldg(R.M2 + (uint64_t)v * W + l) : 0u;
-                m.M4[l] = (l < W) ? __ldg(R.M4 + (uint64_t)v * W + l) : 0u;
-                m.SAT[l] = 0u;
-                m.NC[l] = 0u;
-                m.NX[l] = 0u;
+                if (l == 0) atomicSub(&sp.ctr->busy, 1u);
                 __syncwarp();
-                // saturated members of P + v: neiInP' + k == |P'|
-                for (int i = l; i < (int)np; i += 32) {
-                    const uint32_t u = m.list[i];
-                    const int pu = (int)m.pv[i] + (int)test_bit(m.ROW, u);
-                    if (pu + k == (int)np1) atomicOr(&m.SAT[u >> 5], 1u << (u & 31));
-                }
-                if (l == 0 && (int)m.pv[pidx] + k == (int)np1) atomicOr(&m.SAT[vw], vb);
-                m.P[l] = P1;
-                __syncwarp();
-                // C filter: class >= UNLINK2EQUAL and P'+c a k-plex (isKplex3)
-                for (int i = l; i < (int)nc; i += 32) {
-                    const uint32_t c = m.list[np + i];
-                    if (c == v || !test_bit(m.M2, c)) continue;
-                    const uint32_t* row = R.A + (uint64_t)c * W;
-                    const int pc = (int)m.pv[np + i] + (int)test_bit(m.ROW, c);
-                    if (pc + k < (int)np1 + 1) continue;
-                    bool ok = true;
-                    for (uint32_t w = 0; ok && w < W; ++w) if (m.SAT[w] & ~__ldg(row + w)) ok = false;
-                    if (ok) atomicOr(&m.NC[c >> 5], 1u << (c & 31));
-                }
-                if (l == 0) bb += (unsigned long long)nc * 4ull * W;
-                __syncwarp();
-                const uint32_t C1 = m.NC[l];
-                const uint32_t nc1 = (uint32_t)warp_sum(__popc(C1));
-                m.PC[l] = P1 | C1;
-                __syncwarp();
-                // upperBound2 over P' (src:1022-1040)
-                bool ub = true;
-                for (int i = l; i <= (int)np; i += 32) {
-                    const uint32_t u = (i < (int)np) ? m.list[i] : v;
-                    if (row_and_popc(R.A + (uint64_t)u * W, m.PC, W) + k < q) ub = false;
-                }
-                if (l == 0) bb += (unsigned long long)np1 * 4ull * W;
-                if (!__all_sync(FULL, ub)) break;
-                // X filter: class >= UNLINK2MORE and P'+x a k-plex
-                const int nxl = bits_to_list(Xw, m.list);
-                for (int i = l; i < nxl; i += 32) {
-                    const uint32_t x = m.list[i];
-                    if (!test_bit(m.M4, x)) continue;
-                    const uint32_t* row = R.A + (uint64_t)x * W;
-                    if (row_and_popc(row, m.P, W) + k < (int)np1 + 1) continue;
-                    bool ok = true;
-                    for (uint32_t w = 0; ok && w < W; ++w) if (m.SAT[w] & ~__ldg(row + w)) ok = false;
-                    if (ok) atomicOr(&m.NX[x >> 5], 1u << (x & 31));
-                }
-                if (l == 0) bb += (unsigned long long)nxl * 4ull * W;
-                __syncwarp();
-                const uint32_t X1 = m.NX[l];
-                nx = (uint32_t)warp_sum(__popc(X1));
-                Pw = P1; Cw = C1; Xw = X1;
-                np = np1; nc = nc1;
-                if (l == 0) { ++tasks; bb += 12ull * W; }
-                have_child = true;
-            } while (0);
-            __syncwarp();
-            if (have_child) continue;
-            // next record from this warp's stack
-            if (stop == sbot) { stop = sbot = 0; break; }
-            --stop;
-            const uint32_t* src = stack + (stop % sp.stack_depth) * SW;
-            root = __ldcg(src);
-            const uint32_t h1 = __ldcg(src + 1);
-            np = h1 & 0xffff; nc = h1 >> 16; nx = __ldcg(src + 2);
-            Pw = (l < Wt) ? __ldcg(src + 4 + l) : 0u;
-            Cw = (l < Wt) ? __ldcg(src + 4 + Wt + l) : 0u;
-            Xw = (l < Wt) ? __ldcg(src + 4 + 2 * Wt + l) : 0u;
-            __syncwarp();
+            }
         }
-        if (l == 0) atomicSub(&sp.ctr->busy, 1u);
-        __syncwarp();
+        // ---------------- idle: exit when nothing is left anywhere
+        int done = 0;
+        if (l == 0) {
+            __threadfence();
+            const unsigned nr = *(volatile unsigned*)&sp.ctr->next_root;
+            const unsigned live = *(volatile unsigned*)&sp.ctr->ks_active;
+            const unsigned long long ps = pool_size(sp);
+            const unsigned b = *(volatile unsigned*)&sp.ctr->busy;
+            done = nr >= sp.nroots && live == 0 && ps == 0 && b == 0;
+        }
+        done = __shfl_sync(FULL, done, 0);
+        if (done && !ks_active) break;
+        if (++idle > sp.spin_limit) {
+            if (l == 0) atomicAdd(&sp.ctr->timeouts, 1u);
+            if (!ks_active) break;
+            paused = false;   // a producer never waits unboundedly for the pool to drain
+            idle = 0;
+        }
+        __nanosleep(idle < 64 ? 100 : 1000);
     }
     if (l == 0) {
-        atomicAdd(&sp.ctr->count, cnt);
-        atomicAdd(&sp.ctr->hash, hsum);
-        atomicAdd(&sp.ctr->tasks, tasks);
-        atomicAdd(&sp.ctr->nodes, nodes);
-        atomicAdd(&sp.ctr->bnb_bytes, bb);
+        atomicAdd(&sp.ctr->count, ww.cnt);
+        atomicAdd(&sp.ctr->hash, ww.hsum);
+        atomicAdd(&sp.ctr->tasks, ww.tasks + ks_tasks);
+        atomicAdd(&sp.ctr->ks_tasks, ks_tasks);
+        atomicAdd(&sp.ctr->nodes, ww.nodes);
+        atomicAdd(&sp.ctr->bnb_bytes, ww.bb);
         atomicAdd(&sp.ctr->bnb_done, 1u);
     }
 }

@@ -91,6 +91,11 @@ __device__ inline bool pool_push(const SearchParams& sp, WordFn word) {
     ok = __shfl_sync(FULL, ok, 0);
     if (!ok) return false;
     pos = __shfl_sync(FULL, pos, 0);
+    if (sp.test_stuck) {   // failure-detection test: claim the slot but never publish it
+        int stuck = 0;
+        if (l == 0) stuck = atomicCAS(&sp.ctr->stuck_once, 0u, 1u) == 0u;
+        if (__shfl_sync(FULL, stuck, 0)) return true;
+    }
     const unsigned long long slot = pos % pool->cap;
     uint32_t* dst = sp.pool_data + slot * sp.slot_words;
     for (unsigned i = l; i < sp.slot_words; i += 32) __stcg(dst + i, word(i));

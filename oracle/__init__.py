@@ -47,6 +47,8 @@ def lib() -> ctypes.CDLL:
                                         u32p, u32p, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32), u32p,
                                         ctypes.POINTER(ctypes.c_uint64)]
         L.oracle_preprocess.restype = ctypes.c_longlong
+        L.oracle_enumerate_shard.argtypes = [u32p, u32p, ctypes.c_uint32, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                             ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(OracleResult)]
         _lib = L
     return _lib
 
@@ -66,6 +68,17 @@ def enumerate_csr(off, adj, k: int, q: int, truss: int = 0, threads: int = 0,
     adj, pa = _u32(adj)
     r = OracleResult()
     rc = lib().oracle_enumerate_csr(po, pa, len(off) - 1, k, q, truss, threads, root_begin, root_end, ctypes.byref(r))
+    if rc:
+        raise RuntimeError(f"oracle failed with {rc}")
+    return r.as_dict()
+
+
+def enumerate_shard(off, adj, k: int, q: int, truss: int, shard_index: int, shard_count: int, threads: int = 0) -> dict:
+    """The roots whose degeneracy rank r has r % shard_count == shard_index (the multi-GPU partition)."""
+    off, po = _u32(off)
+    adj, pa = _u32(adj)
+    r = OracleResult()
+    rc = lib().oracle_enumerate_shard(po, pa, len(off) - 1, k, q, truss, threads, shard_index, shard_count, ctypes.byref(r))
     if rc:
         raise RuntimeError(f"oracle failed with {rc}")
     return r.as_dict()

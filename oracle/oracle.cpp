@@ -692,7 +692,8 @@ static void preprocess(const Graph& g0, const Params& P, Graph& pg, std::vector<
     degeneracy(pg, dpos, dseq);
 }
 
-static Result run(const Graph& g0, const Params& P, int threads, uint64_t root_begin, uint64_t root_end) {
+static Result run(const Graph& g0, const Params& P, int threads, uint64_t root_begin, uint64_t root_end,
+                  uint32_t shard_index = 0, uint32_t shard_count = 1) {
     Result R;
     auto t0 = std::chrono::steady_clock::now();
     Graph pg; std::vector<int> dpos, dseq; std::vector<uint32_t> orig;
@@ -713,6 +714,7 @@ static Result run(const Graph& g0, const Params& P, int threads, uint64_t root_b
 #pragma omp single
     {
         for (uint64_t ri = rb; ri < re; ++ri) {
+            if (shard_count > 1 && ri % shard_count != shard_index) continue;
 #pragma omp task firstprivate(ri, PG, DP, DS, OR, ST, PP, TC, TH, TT)
             {
                 std::shared_ptr<Sub> sub = std::make_shared<Sub>();
@@ -786,6 +788,17 @@ int oracle_enumerate_csr(const uint32_t* off, const uint32_t* adj, uint32_t n, i
     oracle::Graph g = oracle::from_csr(off, adj, n);
     oracle::Params P{k, q, truss};
     oracle::Result R = oracle::run(g, P, threads, root_begin, root_end);
+    *out = oracle_result{R.count, R.hash, R.tasks, R.valid, R.truncated, R.depth_cap, R.too_big,
+                         R.pn, R.pm, R.max_n, R.max_left, R.ms_pre, R.ms_search};
+    return 0;
+}
+
+int oracle_enumerate_shard(const uint32_t* off, const uint32_t* adj, uint32_t n, int k, int q, int truss,
+                           int threads, uint32_t shard_index, uint32_t shard_count, oracle_result* out) {
+    if (k < 2 || q < 1 || shard_count == 0 || shard_index >= shard_count) return 1;
+    oracle::Graph g = oracle::from_csr(off, adj, n);
+    oracle::Params P{k, q, truss};
+    oracle::Result R = oracle::run(g, P, threads, 0, UINT64_MAX, shard_index, shard_count);
     *out = oracle_result{R.count, R.hash, R.tasks, R.valid, R.truncated, R.depth_cap, R.too_big,
                          R.pn, R.pm, R.max_n, R.max_left, R.ms_pre, R.ms_search};
     return 0;

@@ -1,0 +1,102 @@
+"""Device path (through the C ABI) against the oracle and the golden fixtures.
+
+Integer work: every comparison is exact — count, the order-independent hash
+of the sorted vertex sets, and the number of generated tasks (the device
+builds the same search tree as the oracle)."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, dataset
+
+pytestmark = pytest.mark.gpu
+
+
+def golden():
+    with open(os.path.join(GOLDEN, "golden.json")) as f:
+        return json.load(f)
+
+
+def test_small_workload(kp, orc):
+    w = kp.WORKLOADS["small"]
+    off, adj = kp.workload_graph("small")
+    g = kp.enumerate_csr(off, adj, w["k"], w["q"], w["thres"], w["truss"])
+    gold = golden()["workloads"]["small"]
+    assert (g["count"], g["hash"], g["tasks"]) == (gold["count"], gold["hash"], gold["tasks"])
+    assert g["valid_roots"] == gold["valid_roots"] and g["pn"] == gold["pn"]
+    assert g["gpu_launches"] >= 3
+
+
+def test_golden_random_graphs(kp, orc):
+    for c in golden()["random"]:
+        off, adj = orc.random_graph(c["n"], c["p"], c["seed"], [tuple(x) for x in c["planted"]])
+        g = kp.enumerate_csr(off, adj, c["k"], c["q"], truss=c["truss"])
+        assert (g["count"], g["hash"], g["tasks"]) == (c["count"], c["hash"], c["tasks"]), c
+
+
+@pytest.mark.parametrize("k", [2, 3, 4, 5])
+@pytest.mark.parametrize("truss", [0, 1])
+def test_random_vs_oracle(kp, orc, k, truss):
+    for seed in range(6):
+        rng = np.random.default_rng(100 * k + seed)
+        n = int(rng.integers(30, 90))
+        off, adj = orc.random_graph(n, float(rng.uniform(0.05, 0.2)), seed,
+                                    [(int(rng.integers(10, 20)), float(rng.uniform(0.8, 1.0))) for _ in range(3)])
+        for q in (2 * k - 1, 2 * k + 1, 2 * k + 4):
+            g = kp.enumerate_csr(off, adj, k, q, truss=truss)
+            o = orc.enumerate_csr(off, adj, k, q, truss, threads=2)
+            assert (g["count"], g["hash"], g["tasks"]) == (o["count"], o["hash"], o["tasks"]), (seed, k, q)
+
+
+def test_edge_cases(kp):
+    # empty graph, no vertex survives the core, graph too small for any root
+    off = np.zeros(1, np.uint32)
+    adj = np.zeros(0, np.uint32)
+    g = kp.enumerate_csr(off, adj, 2, 8)
+    assert g["count"] == 0 and g["hash"] == 0 and g["pn"] == 0
+    n = 10
+    rows = [[j for j in range(n) if j != i] for i in range(n)]
+    off = np.zeros(n + 1, np.uint32)
+    off[1:] = np.cumsum([len(r) for r in rows])
+    adj = np.concatenate(rows).astype(np.uint32)
+    g = kp.enumerate_csr(off, adj, 2, 11)      # K10 has no 11-vertex k-plex
+    assert g["count"] == 0
+    g = kp.enumerate_csr(off, adj, 2, 10)      # exactly the clique
+    assert g["count"] == 1 and g["valid_roots"] >= 1
+
+
+@pytest.mark.parametrize("key", ["soc-epinions.bin:4:30:0", "email-euall.bin:3:12:0", "email-euall.bin:3:12:1"])
+def test_shipped_datasets(kp, key):
+    fname, k, q, tr = key.split(":")
+    p = dataset(fname)
+    if not p:
+        pytest.skip("dataset not copied (tests/golden/fetch_datasets.sh)")
+    g = kp.enumerate_file(p, int(k), int(q), 0.25, int(tr))
+    gold = golden()["datasets"][key]
+    assert g["count"] == {"soc-epinions.bin": 13172906, "email-euall.bin": 32639016}[fname]   # README.md:142, :144
+    assert (g["count"], g["hash"], g["tasks"]) == (gold["count"], gold["hash"], gold["tasks"])
+
+
+@pytest.mark.parametrize("name", ["epinions", "email"])
+def test_full_size_synthetic(kp, name):
+    gold = golden()["workloads"].get(name)
+    if gold is None:
+        pytest.skip("no oracle fixture for this workload")
+    w = kp.WORKLOADS[name]
+    off, adj = kp.workload_graph(name)
+    g = kp.enumerate_csr(off, adj, w["k"], w["q"], w["thres"], w["truss"])
+    assert (g["count"], g["hash"], g["tasks"]) == (gold["count"], gold["hash"], gold["tasks"])
+
+
+def test_repeat_and_reuse(kp):
+    """Device buffers are cached between calls: repeated searches and a second graph stay exact."""
+    off, adj = kp.workload_graph("small")
+    prep = kp.prepare(off, adj, 2, 8)
+    try:
+        a, b = prep.search(), prep.search()
+        assert (a["count"], a["hash"], a["tasks"]) == (b["count"], b["hash"], b["tasks"])
+    finally:
+        prep.release()
+    g = golden()["random"][0]

@@ -1,0 +1,82 @@
+"""Pause-and-resume, root sharding and failure detection on the device.
+
+Failures are made on the host or by bounded waits that give up; nothing here
+faults, traps or hangs the GPU."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _dense(orc):
+    return orc.random_graph(80, 0.15, 3, [(20, 0.9), (18, 0.95), (16, 1.0)])
+
+
+@pytest.mark.parametrize("slots,thres", [(64, 0.5), (256, 0.25), (4096, 1.0)])
+def test_pause_resume_same_result(kp, orc, slots, thres):
+    """A tiny task pool forces k-search to pause many times; results do not change (host:1094-1122)."""
+    off, adj = _dense(orc)
+    full = kp.enumerate_csr(off, adj, 3, 8)
+    g = kp.enumerate_csr(off, adj, 3, 8, thres=thres, pool_slots=slots)
+    assert (g["count"], g["hash"], g["tasks"]) == (full["count"], full["hash"], full["tasks"])
+    if slots == 64:
+        assert g["pauses"] > 0
+
+
+@pytest.mark.parametrize("shards", [2, 3])
+def test_root_shards_sum_to_whole(kp, orc, shards):
+    """Roots are independent: per-shard counts and hashes add up to the whole run (multi-GPU partition)."""
+    off, adj = kp.workload_graph("small")
+    full = kp.enumerate_csr(off, adj, 2, 8)
+    tot_c = tot_h = tot_v = 0
+    for s in range(shards):
+        g = kp.enumerate_csr(off, adj, 2, 8, shard_index=s, shard_count=shards)
+        tot_c += g["count"]
+        tot_h = (tot_h + g["hash"]) % (1 << 64)
+        tot_v += g["valid_roots"]
+    assert (tot_c, tot_h, tot_v) == (full["count"], full["hash"], full["valid_roots"])
+
+
+def test_bounded_wait_reports_timeout(kp, orc):
+    """Branch warps that give up every wait at once leave records behind: the call
+    returns KPLEX_ERR_TIMEOUT instead of hanging, and the device stays usable."""
+    off, adj = _dense(orc)
+    g = kp.enumerate_csr(off, adj, 3, 8, flags=kp.FLAG_QUIET | kp.FLAG_TEST_NO_WAIT, check=False)
+    assert g["status"] == kp.ERR_TIMEOUT
+    ok = kp.enumerate_csr(off, adj, 3, 8)
+    assert ok["status"] == 0 and ok["count"] > 0
+
+
+def _oversized_graph():
+    """root 0 adjacent to 550 of a 600-clique A; 500 vertices B adjacent to all of A.
+    Root 0 is first in the degeneracy order; C1 = its 550 neighbours, C2 = the other
+    50 A-vertices and all of B (550 common neighbours each) -> 1 + 550 + 550 > 1024."""
+    A = list(range(1, 601))
+    B = list(range(601, 1101))
+    adj = {v: set() for v in range(1101)}
+    def add(a, b):
+        adj[a].add(b); adj[b].add(a)
+    for i in A[:550]:
+        add(0, i)
+    for x in range(len(A)):
+        for y in range(x + 1, len(A)):
+            add(A[x], A[y])
+    for b in B:
+        for a in A:
+            add(a, b)
+    n = 1101
+    off = np.zeros(n + 1, np.uint32)
+    off[1:] = np.cumsum([len(adj[v]) for v in range(n)])
+    flat = np.concatenate([np.array(sorted(adj[v]), np.uint32) for v in range(n)])
+    return off, flat
+
+
+def test_oversized_root_is_an_error(kp):
+    """A root whose 2-hop subgraph exceeds 1024 vertices is beyond the reference's
+    MAX_BLK_SIZE (inc/common.h:8): the reference's 2-hop append (src/device_funcs.cu:255)
+    overruns its buffer there; this returns a status and the device stays usable."""
+    off, adj = _oversized_graph()
+    g = kp.enumerate_csr(off, adj, 2, 20, check=False)
+    assert g["status"] == kp.ERR_CAPACITY
+    small = kp.workload_graph("small")
+    assert kp.enumerate_csr(*small, 2, 8)["count"] > 0
