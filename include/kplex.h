@@ -80,6 +80,9 @@ typedef struct {
     uint64_t bnb_bytes;     /* algorithmic bytes of branch-and-bound: 12W per node and per child
                                record (P, C, X bitsets of W words) + 4W per adjacency row read */
     uint64_t roots_bytes;   /* algorithmic bytes of decomposition: CSR words read + bit matrices written */
+    uint64_t ks_tasks;      /* tasks emitted by k-search (the rest of `tasks` are branch children) */
+    uint64_t stage_copies;  /* root adjacency matrices copied into shared memory */
+    double ks_warp_ms;      /* k-search time summed over producer warps (diagnostic) */
 } kplex_result;
 
 /* A CSR graph owned by the library (kplex_load_bin / kplex_generate). */

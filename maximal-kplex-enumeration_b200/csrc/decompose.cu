@@ -350,6 +350,7 @@ __global__ void __launch_bounds__(256) decompose_kernel(SearchParams sp) {
                     atomicMax(&sp.ctr->max_n, (unsigned)n);
                     atomicMax(&sp.ctr->max_left, (unsigned)nleft);
                     atomicMax(&sp.ctr->max_w, W);
+                    atomicMax(&sp.ctr->max_nw, (unsigned)n * W);
                     // CSR words of every local vertex read once + the root block written once
                     unsigned long long csr = 0;
                     for (int i = 0; i < n; ++i) csr += sp.off[S.blk[i] + 1] - sp.off[S.blk[i]];
@@ -388,5 +389,34 @@ __global__ void __launch_bounds__(256) decompose_kernel(SearchParams sp) {
 }
 
 uint64_t decomp_scratch_words_host(uint32_t pn) { return decomp_scratch_words(pn); }
+
+// k-search job prefix: a valid root with |C2| = n - hop owns |C2| + 1 jobs;
+// job_base[r] = jobs of roots < r, job_base[nroots] = total.  One block.
+__global__ void __launch_bounds__(1024) job_prefix_kernel(const RootDesc* roots, uint32_t nroots, uint32_t* job_base) {
+    __shared__ uint32_t part[1024];
+    const uint32_t t = threadIdx.x, T = blockDim.x;
+    const uint32_t per = (nroots + T - 1) / T;
+    const uint32_t b = t * per, e = min(nroots, b + per);
+    uint32_t sum = 0;
+    for (uint32_t r = b; r < e; ++r) {
+        const RootDesc& rd = roots[r];
+        sum += ((rd.flags & ROOT_VALID) && rd.n) ? rd.n - rd.hop + 1 : 0u;
+    }
+    part[t] = sum;
+    __syncthreads();
+    for (uint32_t o = 1; o < T; o <<= 1) {   // inclusive Hillis-Steele scan
+        const uint32_t v = t >= o ? part[t - o] : 0u;
+        __syncthreads();
+        part[t] += v;
+        __syncthreads();
+    }
+    uint32_t run = t ? part[t - 1] : 0u;
+    for (uint32_t r = b; r < e; ++r) {
+        job_base[r] = run;
+        const RootDesc& rd = roots[r];
+        run += ((rd.flags & ROOT_VALID) && rd.n) ? rd.n - rd.hop + 1 : 0u;
+    }
+    if (t == T - 1) job_base[nroots] = part[T - 1];
+}
 
 }  // namespace kplex

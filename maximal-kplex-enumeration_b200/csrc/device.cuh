@@ -59,20 +59,22 @@ struct Counters {
     unsigned long long bnb_bytes;  // algorithmic bytes of branch nodes (roofline accounting)
     unsigned long long arena_top;  // words bump-allocated in the arena
     unsigned int valid_roots;
-    unsigned int max_n, max_left, max_w;
+    unsigned int max_n, max_left, max_w, max_nw;
     unsigned int truncated, oversized, depth_capped;
     unsigned int error;            // KPLEX_ERR_* raised on the device (first one wins)
-    unsigned int next_root;        // k-search root dispenser
+    unsigned int next_root;        // k-search job dispenser
     unsigned int ks_paused;        // k-search warps that stopped at the pause threshold
     unsigned int ks_active;        // k-search slots holding an unfinished root
     unsigned int busy;             // branch warps holding work (termination detection)
     unsigned int bnb_done;         // branch warps that exited
     unsigned int timeouts;         // bounded waits that gave up
     unsigned int decomp_next;      // decomposition root dispenser
-    unsigned int pad[3];
+    unsigned int pad[2];
     unsigned long long roots_bytes; // algorithmic bytes of the decomposition
     unsigned long long ks_tasks;   // tasks emitted by k-search
     unsigned int stuck_once;       // test hook: one pool slot claimed and never published
+    unsigned long long stage_copies;  // adjacency matrices copied to shared memory
+    unsigned long long ks_cycles;  // SM cycles producers spent in k-search
 };
 
 // Vyukov bounded MPMC ring: each slot carries a sequence number so that a
@@ -113,6 +115,10 @@ struct SearchParams {
     uint32_t hash_on;
     uint32_t shard_index, shard_count;
     uint32_t test_stuck;       // test hook: the first push claims a slot and never publishes it
+    uint32_t a_words;          // per-warp shared-memory copy of a root's A (0: read A from the arena)
+    uint32_t stage_after;      // nodes on one root before its A is copied to shared memory
+    const uint32_t* job_base;  // k-search jobs: root r owns jobs [job_base[r], job_base[r+1])
+    uint32_t njobs;
     unsigned long long spin_limit;   // iterations for any bounded wait
 };
 

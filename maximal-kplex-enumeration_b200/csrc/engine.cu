@@ -29,10 +29,12 @@
 namespace kplex {
 
 __global__ void decompose_kernel(SearchParams sp);
-__global__ void search_kernel(SearchParams sp, uint32_t nmax);
+__global__ void search_kernel_3(SearchParams sp, uint32_t nmax);
+__global__ void search_kernel_2(SearchParams sp, uint32_t nmax);
+__global__ void job_prefix_kernel(const RootDesc* roots, uint32_t nroots, uint32_t* job_base);
 uint64_t decomp_scratch_words_host(uint32_t pn);
-uint32_t bnb_smem_words_host(uint32_t nmax, uint32_t slot_words);
-uint32_t ks_slot_words_host();
+uint32_t bnb_smem_words_host(uint32_t nmax, uint32_t slot_words, uint32_t a_words);
+uint32_t ks_slot_words_host(uint32_t nmax);
 
 // ------------------------------------------------------------------ small kernels
 __global__ void init_decomp_scratch(uint32_t* scratch, uint64_t words_per_warp, uint32_t pn, uint32_t nwarps) {
@@ -83,7 +85,7 @@ struct DeviceState {
     bool init = false;
     int sms = 0;
     cudaStream_t stream = nullptr;
-    DevBuf roots, ctr, scratch, arena, pool_seq, pool_data, pool, ks, stacks;
+    DevBuf roots, ctr, scratch, arena, pool_seq, pool_data, pool, ks, stacks, jobs;
     Counters* h_ctr = nullptr;   // pinned
 };
 
@@ -108,6 +110,8 @@ static int device_state(int device, DeviceState** out) {
     *out = &d;
     return KPLEX_OK;
 }
+
+void set_last_error(const std::string& msg) { g_last_error = msg; }
 
 static double ms_since(std::chrono::steady_clock::time_point t0) {
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
@@ -260,6 +264,15 @@ static int search_impl(kplex_prepared* h, kplex_result* out) {
         g_last_error = hc.error == KPLEX_ERR_CAPACITY ? "a root's 2-hop subgraph or left set exceeds 1024 vertices" : "device error in decomposition";
         return (int)hc.error;
     }
+    // k-search jobs: a valid root with |C2| = n - hop owns |C2| + 1 independent jobs
+    if ((rc = d->jobs.ensure(((size_t)nroots + 1) * 4))) return rc;
+    sp.job_base = d->jobs.as<uint32_t>();
+    job_prefix_kernel<<<1, 1024, 0, st>>>(sp.roots, nroots, d->jobs.as<uint32_t>());
+    ++launches;
+    uint32_t njobs = 0;
+    CK(cudaMemcpyAsync(&njobs, d->jobs.as<uint32_t>() + nroots, 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    sp.njobs = njobs;
     const uint32_t nmax = std::max<uint32_t>(hc.max_n, 1);
     const uint32_t Wt = std::max<uint32_t>(hc.max_w, 4);
     sp.Wt = Wt;
@@ -275,12 +288,25 @@ static int search_impl(kplex_prepared* h, kplex_result* out) {
     sp.pool_data = d->pool_data.as<uint32_t>();
     init_pool<<<d->sms * 4, 256, 0, st>>>(sp.pool_seq, cap, sp.pool);
     ++launches;
-    const uint32_t smem_words = ks_slot_words_host() + 8 * bnb_smem_words_host(nmax, sp.slot_words);
     const int warps_per_block = 8;
-    const size_t smem_bytes = (size_t)smem_words * 4;
-    CK(cudaFuncSetAttribute(search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes));
+    // tuning knobs (environment): blocks per SM the kernel is compiled for (2 or 3) and
+    // how many nodes a warp processes on one root before copying its A to shared memory
+    const char* eb = getenv("KPLEX_BLOCKS_PER_SM");
+    const int minb = (eb && atoi(eb) == 2) ? 2 : 3;
+    const char* es = getenv("KPLEX_STAGE_AFTER");
+    sp.stage_after = es ? (uint32_t)atoi(es) : 8u;
+    auto kfn = minb == 2 ? search_kernel_2 : search_kernel_3;
+    // stage adjacency matrices in shared memory when minb 8-warp blocks still fit on an SM
     int per_sm = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, search_kernel, warps_per_block * 32, smem_bytes));
+    size_t smem_bytes = 0;
+    for (int stage = sp.stage_after ? 1 : 0; stage >= 0; --stage) {
+        sp.a_words = stage ? ((hc.max_nw + 3u) & ~3u) : 0u;
+        smem_bytes = (size_t)(ks_slot_words_host(nmax) + warps_per_block * bnb_smem_words_host(nmax, sp.slot_words, sp.a_words)) * 4;
+        if (smem_bytes > 227 * 1024) continue;
+        CK(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, warps_per_block * 32, smem_bytes));
+        if (per_sm >= minb || !stage) break;
+    }
     per_sm = std::max(per_sm, 1);
     const uint32_t blocks = (uint32_t)d->sms * (uint32_t)per_sm;
     const uint32_t nwarps = blocks * warps_per_block;
@@ -299,7 +325,7 @@ static int search_impl(kplex_prepared* h, kplex_result* out) {
 
     // ---------------- k-search + branch-and-bound, one persistent launch
     if (nroots) {
-        if ((rc = timed([&] { search_kernel<<<blocks, warps_per_block * 32, smem_bytes, st>>>(sp, nmax); }, ms_bnb))) return rc;
+        if ((rc = timed([&] { kfn<<<blocks, warps_per_block * 32, smem_bytes, st>>>(sp, nmax); }, ms_bnb))) return rc;
         ++launches;
     }
     CK(cudaMemcpyAsync(&hc, sp.ctr, sizeof(Counters), cudaMemcpyDeviceToHost, st));
@@ -336,6 +362,9 @@ static int search_impl(kplex_prepared* h, kplex_result* out) {
         out->ms_bnb = ms_bnb;
         out->bnb_bytes = hc.bnb_bytes;
         out->roots_bytes = hc.roots_bytes;
+        out->ks_tasks = hc.ks_tasks;
+        out->stage_copies = hc.stage_copies;
+        out->ks_warp_ms = (double)hc.ks_cycles / (1.965e6);   // SM cycles at the 1965 MHz boost clock
         out->status = (int)hc.error;
     }
     return (int)hc.error;

@@ -54,16 +54,28 @@ __device__ __forceinline__ RootView root_view(const SearchParams& sp, uint32_t r
 }
 
 // ============================================================== k-search state (shared memory)
-constexpr int KS_HDR = 8;                         // root, sz, np, nc2
-constexpr int KS_P = KS_HDR;                      // MAX_K words: P stack (local ids, inclusion order)
-constexpr int KS_FR = KS_P + MAX_K;               // KS_MAX_DEPTH frames (+ slack)
-constexpr int KS_C2 = KS_FR + KS_MAX_DEPTH + 8;   // MAX_LOCAL u16: C2 list in the reference's order
-constexpr int KS_T1 = KS_C2 + MAX_LOCAL / 2;      // MAX_LOCAL u16: drop tags of C1 (depth + 1)
-constexpr int KS_T2 = KS_T1 + MAX_LOCAL / 2;      // MAX_LOCAL u16: drop tags of C2
-constexpr int KS_LST = KS_T2 + MAX_LOCAL / 2;     // MAX_LOCAL u16: C1 members (isKplex2 filter)
-constexpr int KS_BITS = KS_LST + MAX_LOCAL / 2;   // C1, X, P bitsets (32 words each)
-constexpr int KS_AUX = KS_BITS + 3 * MAX_WORDS;   // three 32-word scratch masks
-constexpr int KS_WORDS = KS_AUX + 3 * MAX_WORDS;
+// Layout in words, sized by the largest root n_max of the search:
+//   hdr (root, sz, np, nc2) | P stack [MAX_K] | frames | C2 list | C1 tags | C2 tags |
+//   C1 member list | C1, X, P bitsets [3 x 32] | scratch masks [3 x 32]
+// Along any stack path every pushed frame moves one C2 vertex to X or P (the
+// last push may add one leaf frame), so min(n_max + 8, KS_MAX_DEPTH + 8) frames suffice.
+struct KsLayout { uint32_t fr, c2, t1, t2, lst, bits, aux, total; };
+
+__host__ __device__ inline KsLayout ks_layout(uint32_t nmax) {
+    KsLayout L;
+    uint32_t o = 8 + MAX_K;
+    const uint32_t frames = ((nmax + 8 < (uint32_t)KS_MAX_DEPTH + 8 ? nmax + 8 : (uint32_t)KS_MAX_DEPTH + 8) + 3u) & ~3u;
+    const uint32_t half = (((nmax + 1) / 2) + 3u) & ~3u;
+    L.fr = o; o += frames;
+    L.c2 = o; o += half;
+    L.t1 = o; o += half;
+    L.t2 = o; o += half;
+    L.lst = o; o += half;
+    L.bits = o; o += 3 * MAX_WORDS;
+    L.aux = o; o += 3 * MAX_WORDS;
+    L.total = o;
+    return L;
+}
 
 // frame: res (8) | br (8) | state (4) | v2delete (12)
 __device__ __forceinline__ uint32_t fr_pack(uint32_t res, uint32_t br, uint32_t st, uint32_t v) {
@@ -76,43 +88,60 @@ __device__ __forceinline__ uint32_t fr_v(uint32_t f) { return f >> 20; }
 
 struct KsSlot {
     uint32_t* w;
+    KsLayout L;
     __device__ uint32_t& root() const { return w[0]; }
     __device__ uint32_t& sz() const { return w[1]; }
     __device__ uint32_t& np() const { return w[2]; }
     __device__ uint32_t& nc2() const { return w[3]; }
-    __device__ uint32_t* P() const { return w + KS_P; }
-    __device__ uint32_t* fr() const { return w + KS_FR; }
-    __device__ uint16_t* c2() const { return reinterpret_cast<uint16_t*>(w + KS_C2); }
-    __device__ uint16_t* t1() const { return reinterpret_cast<uint16_t*>(w + KS_T1); }
-    __device__ uint16_t* t2() const { return reinterpret_cast<uint16_t*>(w + KS_T2); }
-    __device__ uint16_t* lst() const { return reinterpret_cast<uint16_t*>(w + KS_LST); }
-    __device__ uint32_t* bits() const { return w + KS_BITS; }
-    __device__ uint32_t* mask() const { return w + KS_AUX; }
-    __device__ uint32_t* aux() const { return w + KS_AUX + MAX_WORDS; }
-    __device__ uint32_t* keep() const { return w + KS_AUX + 2 * MAX_WORDS; }
+    __device__ uint32_t* P() const { return w + 8; }
+    __device__ uint32_t* fr() const { return w + L.fr; }
+    __device__ uint16_t* c2() const { return reinterpret_cast<uint16_t*>(w + L.c2); }
+    __device__ uint16_t* t1() const { return reinterpret_cast<uint16_t*>(w + L.t1); }
+    __device__ uint16_t* t2() const { return reinterpret_cast<uint16_t*>(w + L.t2); }
+    __device__ uint16_t* lst() const { return reinterpret_cast<uint16_t*>(w + L.lst); }
+    __device__ uint32_t* bits() const { return w + L.bits; }
+    __device__ uint32_t* mask() const { return w + L.aux; }
+    __device__ uint32_t* aux() const { return w + L.aux + MAX_WORDS; }
+    __device__ uint32_t* keep() const { return w + L.aux + 2 * MAX_WORDS; }
 };
 
-// Initial sets for root r (src:447-460, 1953-1975): P = {0}, C1 = [1,hop), C2 = [hop,n), X = {}.
-__device__ void ks_start(const SearchParams& sp, const KsSlot& S, uint32_t r, const RootDesc& d) {
+// Initial state of k-search job (r, d).  The reference's k-search for a root
+// (src:1993-2442, from the initial sets of src:447-460 and 1953-1975:
+// P = {0}, C1 = [1,hop), C2 = [hop,n) in ascending order) starts with an
+// exclude chain: state 0 moves the last C2 vertex to X and pushes a child, m
+// times for |C2| = m, with no inclusion in between.  The frame at chain depth
+// d therefore sees P = {0}, C1 = [1,hop), C2 = the first m-d vertices and
+// X = the last d.  When its exclude child returns (state 1) it puts its vertex
+// back and runs its include branches (state 2, br = 1).  Job d < m is exactly
+// that frame from state 2 on; job m is the chain's bottom (C2 empty, state 0).
+// The jobs are independent, so one root's k-search spreads over many warps,
+// and their emissions are the reference's emissions for the root.
+__device__ void ks_start(const SearchParams& sp, const KsSlot& S, uint32_t r, uint32_t d, const RootDesc& rd) {
     const unsigned l = lane_id();
-    const uint32_t n = d.n, hop = d.hop;
+    const uint32_t n = rd.n, hop = rd.hop, m = n - hop;
+    const uint32_t keep = m - d;   // C2 list = [hop, hop + keep), X = [hop + keep, n)
     const uint32_t lo = l * 32;
-    uint32_t c1 = 0;
-    for (uint32_t b = 0; b < 32; ++b) { const uint32_t v = lo + b; if (v >= 1 && v < hop) c1 |= 1u << b; }
+    uint32_t c1 = 0, x = 0;
+    for (uint32_t b = 0; b < 32; ++b) {
+        const uint32_t v = lo + b;
+        if (v >= 1 && v < hop) c1 |= 1u << b;
+        if (v >= hop + keep && v < n) x |= 1u << b;
+    }
     S.bits()[l] = c1;
-    S.bits()[MAX_WORDS + l] = 0u;
+    S.bits()[MAX_WORDS + l] = x;
     S.bits()[2 * MAX_WORDS + l] = (l == 0) ? 1u : 0u;
     for (uint32_t i = l; i < n; i += 32) {
-        if (i >= hop) S.c2()[i - hop] = (uint16_t)i;
+        if (i >= hop && i < hop + keep) S.c2()[i - hop] = (uint16_t)i;
         S.t1()[i] = 0;
         S.t2()[i] = 0;
     }
     if (l == 0) {
         S.P()[0] = 0;
         S.np() = 1;
-        S.nc2() = n - hop;
+        S.nc2() = keep;
         S.sz() = 1;
-        S.fr()[0] = fr_pack((uint32_t)(sp.k - 1), 1, 0, 0);
+        S.w[4] = d;   // chain depth: the frame's depth in the reference's stack
+        S.fr()[0] = fr_pack((uint32_t)(sp.k - 1), 1, d < m ? 2u : 0u, 0);
         S.root() = r;
     }
     __syncwarp();
@@ -189,8 +218,10 @@ __device__ int ks_advance(const SearchParams& sp, const KsSlot& S, Emitted* e) {
     auto setfr = [&](uint32_t f, uint32_t val) { __syncwarp(); if (l == 0) S.fr()[f] = val; __syncwarp(); };
 
     while (sz && !emitted) {
-        if (sz >= (uint32_t)KS_MAX_DEPTH) {   // src:1987-1991: the reference abandons the root
-            if (l == 0) atomicAdd(&sp.ctr->depth_capped, 1u);
+        if (sz + S.w[4] >= (uint32_t)KS_MAX_DEPTH) {
+            // src:1987-1991: the reference abandons the rest of the root at this depth; with
+            // the root split into jobs that cut is not reproducible, so the run reports it
+            if (l == 0) { atomicAdd(&sp.ctr->depth_capped, 1u); raise_error(sp.ctr, KPLEX_ERR_CAPACITY); }
             sz = 0;
             break;
         }
@@ -310,6 +341,35 @@ __device__ int ks_advance(const SearchParams& sp, const KsSlot& S, Emitted* e) {
 }
 
 // ============================================================== branch-and-bound
+// Adjacency rows are read through a generic pointer: the warp's copy of the
+// root's A in shared memory when it fits, else the arena in global memory.
+__device__ __forceinline__ int rowg_popc(const uint32_t* row, const uint32_t* mask, unsigned W) {
+    int c = 0;
+    const uint4* r4 = reinterpret_cast<const uint4*>(row);
+    const uint4* m4 = reinterpret_cast<const uint4*>(mask);
+    for (unsigned w = 0; w < W / 4; ++w) {
+        const uint4 a = r4[w], m = m4[w];
+        c += __popc(a.x & m.x) + __popc(a.y & m.y) + __popc(a.z & m.z) + __popc(a.w & m.w);
+    }
+    return c;
+}
+// popcount of row & mask, and whether every bit of sat is in row
+__device__ __forceinline__ int rowg_popc_covers(const uint32_t* row, const uint32_t* mask, const uint32_t* sat,
+                                                unsigned W, bool* covers) {
+    int c = 0;
+    uint32_t miss = 0;
+    const uint4* r4 = reinterpret_cast<const uint4*>(row);
+    const uint4* m4 = reinterpret_cast<const uint4*>(mask);
+    const uint4* s4 = reinterpret_cast<const uint4*>(sat);
+    for (unsigned w = 0; w < W / 4; ++w) {
+        const uint4 a = r4[w], m = m4[w], t = s4[w];
+        c += __popc(a.x & m.x) + __popc(a.y & m.y) + __popc(a.z & m.z) + __popc(a.w & m.w);
+        miss |= (t.x & ~a.x) | (t.y & ~a.y) | (t.z & ~a.z) | (t.w & ~a.w);
+    }
+    *covers = (miss == 0);
+    return c;
+}
+
 struct BnbSmem {
     uint32_t* rec;    // slot_words: record being loaded from the pool
     uint32_t* P;      // 32 words each
@@ -324,11 +384,12 @@ struct BnbSmem {
     uint16_t* list;   // nmax
     uint16_t* gv;     // nmax
     uint16_t* pv;     // nmax
+    uint32_t* A;      // a_words: the current root's adjacency matrix, when it fits
 };
 
-__host__ __device__ inline uint32_t bnb_smem_words(uint32_t nmax, uint32_t slot_words) {
+__host__ __device__ inline uint32_t bnb_smem_words(uint32_t nmax, uint32_t slot_words, uint32_t a_words) {
     const uint32_t lists = 3 * ((nmax + 1) / 2);
-    return ((slot_words + 9 * MAX_WORDS + lists) + 3u) & ~3u;
+    return (((slot_words + 9 * MAX_WORDS + lists) + 3u) & ~3u) + a_words;
 }
 
 __device__ inline BnbSmem bnb_smem(uint32_t* base, uint32_t nmax, uint32_t slot_words) {
@@ -346,7 +407,8 @@ __device__ inline BnbSmem bnb_smem(uint32_t* base, uint32_t nmax, uint32_t slot_
     m.SB = p; p += MAX_WORDS;
     m.list = reinterpret_cast<uint16_t*>(p); p += (nmax + 1) / 2;
     m.gv = reinterpret_cast<uint16_t*>(p); p += (nmax + 1) / 2;
-    m.pv = reinterpret_cast<uint16_t*>(p);
+    m.pv = reinterpret_cast<uint16_t*>(p); p += (nmax + 1) / 2;
+    m.A = base + (((slot_words + 9 * MAX_WORDS + 3 * ((nmax + 1) / 2)) + 3u) & ~3u);
     return m;
 }
 
@@ -456,7 +518,7 @@ struct WarpWork {
 // One branch-and-bound node (BNB, src:1516-1724).  Returns true when the node
 // produced an include child, which is left in *t; the exclude child is pushed
 // on the warp's stack.
-__device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootView& R, Node* t, WarpWork& ww) {
+__device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootView& R, const uint32_t* A, Node* t, WarpWork& ww) {
     const unsigned l = lane_id();
     const int k = sp.k, q = sp.q;
     const uint32_t W = R.W, Wt = sp.Wt, SW = sp.slot_words;
@@ -470,9 +532,9 @@ __device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootVie
     bits_to_list(Cw, m.list + np);
     const int tot = (int)(np + nc);
     for (int i = l; i < tot; i += 32) {
-        const uint32_t* row = R.A + (uint64_t)m.list[i] * W;
-        m.gv[i] = (uint16_t)row_and_popc(row, m.PC, W);
-        m.pv[i] = (uint16_t)row_and_popc(row, m.P, W);
+        const uint32_t* row = A + (uint32_t)m.list[i] * W;
+        m.gv[i] = (uint16_t)rowg_popc(row, m.PC, W);
+        m.pv[i] = (uint16_t)rowg_popc(row, m.P, W);
     }
     if (l == 0) ww.bb += (unsigned long long)(tot + 3) * 4ull * W;   // rows + the record's P, C, X
     __syncwarp();
@@ -496,7 +558,7 @@ __device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootVie
     int piv, pmin, pval, pidx;
     if (minP + k < tot) {
         // candidates not adjacent to the P pivot (src:1626-1663)
-        m.ROW[l] = (l < W) ? __ldg(R.A + (uint64_t)pp * W + l) : 0u;
+        m.ROW[l] = (l < W) ? A[(uint32_t)pp * W + l] : 0u;
         __syncwarp();
         pmin = INT_MAX; piv = -1; pval = 0; pidx = -1;
         for (int i = l; i < (int)nc; i += 32) {
@@ -522,7 +584,7 @@ __device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootVie
             if (tot < q) return false;
             const int nxl = bits_to_list(Xw, m.list + tot);
             for (int i = l; i < nxl; i += 32)
-                m.gv[tot + i] = (uint16_t)row_and_popc(R.A + (uint64_t)m.list[tot + i] * W, m.PC, W);
+                m.gv[tot + i] = (uint16_t)rowg_popc(A + (uint32_t)m.list[tot + i] * W, m.PC, W);
             m.SAT[l] = 0u;
             __syncwarp();
             for (int i = l; i < tot; i += 32)
@@ -531,9 +593,8 @@ __device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootVie
             bool ext = false;
             for (int i = l; i < nxl; i += 32) {   // isKplexPC2 src:601-622
                 if ((int)m.gv[tot + i] + k < tot + 1) continue;
-                const uint32_t* row = R.A + (uint64_t)m.list[tot + i] * W;
-                bool ok = true;
-                for (uint32_t w = 0; ok && w < W; ++w) if (m.SAT[w] & ~__ldg(row + w)) ok = false;
+                bool ok;
+                rowg_popc_covers(A + (uint32_t)m.list[tot + i] * W, m.SAT, m.SAT, W, &ok);
                 ext |= ok;
             }
             if (l == 0) ww.bb += (unsigned long long)nxl * 4ull * W;
@@ -559,7 +620,7 @@ __device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootVie
     // include child
     const uint32_t np1 = np + 1;
     const uint32_t P1 = (l == vw) ? (Pw | vb) : Pw;
-    m.ROW[l] = (l < W) ? __ldg(R.A + (uint64_t)v * W + l) : 0u;
+    m.ROW[l] = (l < W) ? A[v * W + l] : 0u;
     m.M2[l] = (l < W) ? __ldg(R.M2 + (uint64_t)v * W + l) : 0u;
     m.M4[l] = (l < W) ? __ldg(R.M4 + (uint64_t)v * W + l) : 0u;
     m.SAT[l] = 0u;
@@ -579,11 +640,10 @@ __device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootVie
     for (int i = l; i < (int)nc; i += 32) {
         const uint32_t c = m.list[np + i];
         if (c == v || !test_bit(m.M2, c)) continue;
-        const uint32_t* row = R.A + (uint64_t)c * W;
         const int pc = (int)m.pv[np + i] + (int)test_bit(m.ROW, c);
         if (pc + k < (int)np1 + 1) continue;
-        bool ok = true;
-        for (uint32_t w = 0; ok && w < W; ++w) if (m.SAT[w] & ~__ldg(row + w)) ok = false;
+        bool ok;
+        rowg_popc_covers(A + c * W, m.SAT, m.SAT, W, &ok);
         if (ok) atomicOr(&m.NC[c >> 5], 1u << (c & 31));
     }
     if (l == 0) ww.bb += (unsigned long long)nc * 4ull * W;
@@ -596,7 +656,7 @@ __device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootVie
     bool ub = true;
     for (int i = l; i <= (int)np; i += 32) {
         const uint32_t u = (i < (int)np) ? m.list[i] : v;
-        if (row_and_popc(R.A + (uint64_t)u * W, m.PC, W) + k < q) ub = false;
+        if (rowg_popc(A + u * W, m.PC, W) + k < q) ub = false;
     }
     if (l == 0) ww.bb += (unsigned long long)np1 * 4ull * W;
     if (!__all_sync(FULL, ub)) return false;
@@ -605,11 +665,9 @@ __device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootVie
     for (int i = l; i < nxl; i += 32) {
         const uint32_t x = m.list[i];
         if (!test_bit(m.M4, x)) continue;
-        const uint32_t* row = R.A + (uint64_t)x * W;
-        if (row_and_popc(row, m.P, W) + k < (int)np1 + 1) continue;
-        bool ok = true;
-        for (uint32_t w = 0; ok && w < W; ++w) if (m.SAT[w] & ~__ldg(row + w)) ok = false;
-        if (ok) atomicOr(&m.NX[x >> 5], 1u << (x & 31));
+        bool ok;
+        const int px = rowg_popc_covers(A + x * W, m.P, m.SAT, W, &ok);
+        if (ok && px + k >= (int)np1 + 1) atomicOr(&m.NX[x >> 5], 1u << (x & 31));
     }
     if (l == 0) ww.bb += (unsigned long long)nxl * 4ull * W;
     __syncwarp();
@@ -640,7 +698,7 @@ __device__ __forceinline__ void load_record(const uint32_t* src, uint32_t Wt, No
     }
 }
 
-__global__ void __launch_bounds__(256, 3) search_kernel(SearchParams sp, uint32_t nmax) {
+__device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
     extern __shared__ uint4 smem4[];
     uint32_t* smem = reinterpret_cast<uint32_t*>(smem4);
     const unsigned l = lane_id();
@@ -648,8 +706,12 @@ __global__ void __launch_bounds__(256, 3) search_kernel(SearchParams sp, uint32_
     const unsigned warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t SW = sp.slot_words, Wt = sp.Wt;
     const bool producer = (wib == 0);
-    const KsSlot S{smem};
-    const BnbSmem m = bnb_smem(smem + KS_WORDS + wib * bnb_smem_words(nmax, SW), nmax, SW);
+    const KsLayout KL = ks_layout(nmax);
+    const KsSlot S{smem, KL};
+    const BnbSmem m = bnb_smem(smem + KL.total + wib * bnb_smem_words(nmax, SW, sp.a_words), nmax, SW);
+    const uint32_t* A = nullptr;
+    uint32_t same_root = 0;
+    unsigned long long stage_copies = 0, ks_cycles = 0;
     WarpWork ww;
     ww.stack = sp.stacks + (uint64_t)warp * sp.stack_depth * SW;
     ww.sbot = ww.stop = 0;
@@ -681,9 +743,22 @@ __global__ void __launch_bounds__(256, 3) search_kernel(SearchParams sp, uint32_
                     if (pool_push(sp, [&](unsigned i) { return __ldcg(src + i); })) ++ww.sbot;
                 }
             }
-            if (t.root != cur_root) { R = root_view(sp, t.root); cur_root = t.root; }
+            if (t.root != cur_root) {
+                R = root_view(sp, t.root);
+                cur_root = t.root;
+                A = R.A;
+                same_root = 0;
+            } else if (++same_root == sp.stage_after && R.n * R.W <= sp.a_words) {
+                // the warp keeps working on this root: copy its adjacency rows to shared memory
+                const uint4* src = reinterpret_cast<const uint4*>(R.A);
+                uint4* dst = reinterpret_cast<uint4*>(m.A);
+                for (uint32_t i = l; i < R.n * R.W / 4; i += 32) dst[i] = __ldg(src + i);
+                __syncwarp();
+                A = m.A;
+                ++stage_copies;
+            }
             ++ww.nodes;
-            have = bnb_node(sp, m, R, &t, ww);
+            have = bnb_node(sp, m, R, A, &t, ww);
             __syncwarp();
             if (!have && ww.stop == ww.sbot) {
                 ww.stop = ww.sbot = 0;
@@ -701,25 +776,29 @@ __global__ void __launch_bounds__(256, 3) search_kernel(SearchParams sp, uint32_
             }
             if (!paused) {
                 if (!ks_active) {
-                    // claim the next valid root; ks_active rises before the claim so that
-                    // consumers never see "all roots claimed" with a claim in flight
-                    for (;;) {
-                        int r = -1;
-                        if (l == 0 && *(volatile unsigned*)&sp.ctr->next_root < sp.nroots) {
-                            atomicAdd(&sp.ctr->ks_active, 1u);
-                            const unsigned c = atomicAdd(&sp.ctr->next_root, 1u);
-                            if (c < sp.nroots) r = (int)c;
-                            else atomicSub(&sp.ctr->ks_active, 1u);
-                        }
-                        r = __shfl_sync(FULL, r, 0);
-                        if (r < 0) break;
-                        const RootDesc d = sp.roots[r];
-                        if ((d.flags & ROOT_VALID) && d.n) { ks_start(sp, S, (uint32_t)r, d); ks_active = true; break; }
-                        if (l == 0) atomicSub(&sp.ctr->ks_active, 1u);
+                    // claim the next k-search job; ks_active rises before the claim so that
+                    // consumers never see "all jobs claimed" with a claim in flight
+                    int j = -1;
+                    if (l == 0 && *(volatile unsigned*)&sp.ctr->next_root < sp.njobs) {
+                        atomicAdd(&sp.ctr->ks_active, 1u);
+                        const unsigned c = atomicAdd(&sp.ctr->next_root, 1u);
+                        if (c < sp.njobs) j = (int)c;
+                        else atomicSub(&sp.ctr->ks_active, 1u);
+                    }
+                    j = __shfl_sync(FULL, j, 0);
+                    if (j >= 0) {
+                        // root of job j: the last r with job_base[r] <= j
+                        uint32_t lo2 = 0, hi2 = sp.nroots;
+                        while (hi2 - lo2 > 1) { const uint32_t mid = (lo2 + hi2) >> 1; if (__ldg(sp.job_base + mid) <= (uint32_t)j) lo2 = mid; else hi2 = mid; }
+                        const RootDesc rd = sp.roots[lo2];
+                        ks_start(sp, S, lo2, (uint32_t)j - __ldg(sp.job_base + lo2), rd);
+                        ks_active = true;
                     }
                 }
                 if (ks_active) {
+                    const long long c0 = clock64();
                     const int got = ks_advance(sp, S, &e);
+                    ks_cycles += (unsigned long long)(clock64() - c0);
                     if (got) {
                         ++ks_tasks;
                         const uint32_t r = S.root();
@@ -779,7 +858,7 @@ __global__ void __launch_bounds__(256, 3) search_kernel(SearchParams sp, uint32_
             const unsigned live = *(volatile unsigned*)&sp.ctr->ks_active;
             const unsigned long long ps = pool_size(sp);
             const unsigned b = *(volatile unsigned*)&sp.ctr->busy;
-            done = nr >= sp.nroots && live == 0 && ps == 0 && b == 0;
+            done = nr >= sp.njobs && live == 0 && ps == 0 && b == 0;
         }
         done = __shfl_sync(FULL, done, 0);
         if (done && !ks_active) break;
@@ -799,10 +878,17 @@ __global__ void __launch_bounds__(256, 3) search_kernel(SearchParams sp, uint32_
         atomicAdd(&sp.ctr->nodes, ww.nodes);
         atomicAdd(&sp.ctr->bnb_bytes, ww.bb);
         atomicAdd(&sp.ctr->bnb_done, 1u);
+        atomicAdd(&sp.ctr->stage_copies, stage_copies);
+        atomicAdd(&sp.ctr->ks_cycles, ks_cycles);
     }
 }
 
-uint32_t bnb_smem_words_host(uint32_t nmax, uint32_t slot_words) { return bnb_smem_words(nmax, slot_words); }
-uint32_t ks_slot_words_host() { return (uint32_t)KS_WORDS; }
+// One body, compiled for two register budgets: 3 blocks of 256 threads per SM
+// (80 registers, some spills) or 2 blocks (up to 128 registers).
+__global__ void __launch_bounds__(256, 3) search_kernel_3(SearchParams sp, uint32_t nmax) { search_body(sp, nmax); }
+__global__ void __launch_bounds__(256, 2) search_kernel_2(SearchParams sp, uint32_t nmax) { search_body(sp, nmax); }
+
+uint32_t bnb_smem_words_host(uint32_t nmax, uint32_t slot_words, uint32_t a_words) { return bnb_smem_words(nmax, slot_words, a_words); }
+uint32_t ks_slot_words_host(uint32_t nmax) { return ks_layout(nmax).total; }
 
 }  // namespace kplex

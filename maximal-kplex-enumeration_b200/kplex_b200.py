@@ -41,7 +41,8 @@ class Result(ctypes.Structure):
                 ("spilled", ctypes.c_uint32), ("ms_preprocess", ctypes.c_double), ("ms_device", ctypes.c_double),
                 ("ms_ref_region", ctypes.c_double), ("ms_total", ctypes.c_double), ("status", ctypes.c_int),
                 ("gpu_launches", ctypes.c_uint32), ("ms_decompose", ctypes.c_double), ("ms_ksearch", ctypes.c_double),
-                ("ms_bnb", ctypes.c_double), ("bnb_bytes", ctypes.c_uint64), ("roots_bytes", ctypes.c_uint64)]
+                ("ms_bnb", ctypes.c_double), ("bnb_bytes", ctypes.c_uint64), ("roots_bytes", ctypes.c_uint64),
+                ("ks_tasks", ctypes.c_uint64), ("stage_copies", ctypes.c_uint64), ("ks_warp_ms", ctypes.c_double)]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}

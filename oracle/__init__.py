@@ -47,6 +47,8 @@ def lib() -> ctypes.CDLL:
                                         u32p, u32p, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32), u32p,
                                         ctypes.POINTER(ctypes.c_uint64)]
         L.oracle_preprocess.restype = ctypes.c_longlong
+        L.oracle_enumerate_sequential.argtypes = [u32p, u32p, ctypes.c_uint32, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                  ctypes.c_int, ctypes.POINTER(OracleResult)]
         L.oracle_enumerate_shard.argtypes = [u32p, u32p, ctypes.c_uint32, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                              ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(OracleResult)]
         _lib = L
@@ -68,6 +70,17 @@ def enumerate_csr(off, adj, k: int, q: int, truss: int = 0, threads: int = 0,
     adj, pa = _u32(adj)
     r = OracleResult()
     rc = lib().oracle_enumerate_csr(po, pa, len(off) - 1, k, q, truss, threads, root_begin, root_end, ctypes.byref(r))
+    if rc:
+        raise RuntimeError(f"oracle failed with {rc}")
+    return r.as_dict()
+
+
+def enumerate_sequential(off, adj, k: int, q: int, truss: int = 0, threads: int = 0) -> dict:
+    """As enumerate_csr but with the reference's single sequential k-search per root."""
+    off, po = _u32(off)
+    adj, pa = _u32(adj)
+    r = OracleResult()
+    rc = lib().oracle_enumerate_sequential(po, pa, len(off) - 1, k, q, truss, threads, ctypes.byref(r))
     if rc:
         raise RuntimeError(f"oracle failed with {rc}")
     return r.as_dict()

@@ -32,6 +32,15 @@
 //    writes the already-zero tag; the only observable difference is the final
 //    recovery of the depth-0 frame, which runs after the last emission.
 //  * Counts are 64-bit (the reference's plex_count is u32, src:1585).
+//  * k-search runs each root as |C2|+1 independent jobs, as the device does:
+//    job d is the frame at depth d of the root's initial exclude chain,
+//    started from C2 = its first |C2|-d vertices in ascending order.  The
+//    reference's single state machine reaches that frame with C2 permuted
+//    (finished frames re-append included and recovered vertices at the end,
+//    src:2405-2441), so it lists some subsets under different branches; every
+//    subset S of C2 with |S| <= k-1 is still enumerated exactly once, so the
+//    k-plexes found are the same.  oracle_enumerate_sequential (CLI -seq)
+//    keeps the reference's order.
 // Parity anchors: README.md:142 (soc-epinions k=4 q=30 -> 13,172,906) and
 // README.md:144 (email-euall k=3 q=12 -> 32,639,016), checked by tests/.
 #include <cstdint>
@@ -282,6 +291,7 @@ static bool decompose_root(const Graph& g, const std::vector<int>& dpos, const s
     left.insert(left.end(), left2.begin(), left2.end());
     std::sort(left.begin(), left.end());
     const int n = hop + (int)c2.size();
+    s.n = n; s.nleft = (int)left.size();
     if (n < q) return false;
     st.valid++;
     if (n > MAX_BLK || (int)left.size() > MAX_BLK) { st.too_big++; return false; }
@@ -547,7 +557,7 @@ static void bnb(Ctx& c, Task& t) {
 // src:1855-2444, state machine restated for one root; each emitted task is
 // handed to `sink` (which runs branch-and-bound on it).
 template <typename Sink>
-static void ksearch(const Sub& s, const Params& P, Stats& st, uint64_t& tasks, Sink sink) {
+static void ksearch(const Sub& s, const Params& P, Stats& st, uint64_t& tasks, Sink sink, int job_d = -1) {
     const int n = s.n, k = P.k, q = P.q, hop = s.hop;
     std::vector<uint16_t> G(n), Pn(n, 0);
     for (int i = 0; i < n; ++i) G[i] = (uint16_t)s.degHop[i];
@@ -592,8 +602,17 @@ static void ksearch(const Sub& s, const Params& P, Stats& st, uint64_t& tasks, S
     };
     int sz = 0;
     res[0] = k - 1; br[0] = 1; state[0] = 0; sz = 1;
+    int depth_off = 0;
+    if (job_d >= 0) {
+        // job d of the root (see ks_start in the device code): the exclude-chain frame at
+        // depth d, from state 2 (d < |C2|) or the chain's bottom leaf (d == |C2|)
+        const int m = n - hop;
+        for (int i = 0; i < job_d; ++i) { excl.push_back(cand2.back()); cand2.pop_back(); }
+        state[0] = job_d < m ? 2 : 0;
+        depth_off = job_d;
+    }
     while (sz) {
-        if (sz >= MAX_DEPTH) { st.depth_cap++; break; }
+        if (sz + depth_off >= MAX_DEPTH) { st.depth_cap++; break; }
         const int f = sz - 1;
         const int tag = f + 1;
         switch (state[f]) {
@@ -693,7 +712,7 @@ static void preprocess(const Graph& g0, const Params& P, Graph& pg, std::vector<
 }
 
 static Result run(const Graph& g0, const Params& P, int threads, uint64_t root_begin, uint64_t root_end,
-                  uint32_t shard_index = 0, uint32_t shard_count = 1) {
+                  uint32_t shard_index = 0, uint32_t shard_count = 1, bool sequential_ksearch = false) {
     Result R;
     auto t0 = std::chrono::steady_clock::now();
     Graph pg; std::vector<int> dpos, dseq; std::vector<uint32_t> orig;
@@ -710,18 +729,21 @@ static Result run(const Graph& g0, const Params& P, int threads, uint64_t root_b
     const Graph* PG = &pg; const std::vector<int>* DP = &dpos; const std::vector<int>* DS = &dseq;
     const std::vector<uint32_t>* OR = &orig; Stats* ST = &st; const Params* PP = &P;
     std::atomic<uint64_t>* TC = &tot_cnt; std::atomic<uint64_t>* TH = &tot_hash; std::atomic<uint64_t>* TT = &tot_tasks;
+    const bool seq = sequential_ksearch;
 #pragma omp parallel
 #pragma omp single
     {
         for (uint64_t ri = rb; ri < re; ++ri) {
             if (shard_count > 1 && ri % shard_count != shard_index) continue;
-#pragma omp task firstprivate(ri, PG, DP, DS, OR, ST, PP, TC, TH, TT)
+#pragma omp task firstprivate(ri, PG, DP, DS, OR, ST, PP, TC, TH, TT, seq)
             {
                 std::shared_ptr<Sub> sub = std::make_shared<Sub>();
                 if (decompose_root(*PG, *DP, *DS, (uint32_t)ri, *PP, *sub, *ST)) {
                     uint64_t kt = 0;
                     std::vector<std::shared_ptr<Task>> produced;
-                    ksearch(*sub, *PP, *ST, kt, [&produced](Task& t) { produced.push_back(std::make_shared<Task>(std::move(t))); });
+                    auto keep = [&produced](Task& t) { produced.push_back(std::make_shared<Task>(std::move(t))); };
+                    if (seq) ksearch(*sub, *PP, *ST, kt, keep);
+                    else for (int d = 0; d <= sub->n - sub->hop; ++d) ksearch(*sub, *PP, *ST, kt, keep, d);
                     *TT += kt;
                     for (auto& tp : produced) {
 #pragma omp task firstprivate(tp, sub, OR, ST, PP, TC, TH, TT)
@@ -804,6 +826,73 @@ int oracle_enumerate_shard(const uint32_t* off, const uint32_t* adj, uint32_t n,
     return 0;
 }
 
+// Checks that the |C2|+1 k-search jobs of every root emit exactly the tasks of
+// the sequential k-search (as multisets of label arrays).  Returns the number
+// of roots that differ.
+long long oracle_check_ksearch_jobs(const uint32_t* off, const uint32_t* adj, uint32_t n, int k, int q, int truss) {
+    oracle::Graph g = oracle::from_csr(off, adj, n), pg;
+    oracle::Params P{k, q, truss};
+    std::vector<int> dpos, dseq; std::vector<uint32_t> orig;
+    oracle::preprocess(g, P, pg, dpos, dseq, orig);
+    const long long lim = (long long)pg.n - q + 2;
+    const uint64_t nroots = lim > 0 ? (uint64_t)lim : 0;
+    oracle::Stats st;
+    std::atomic<long long> bad{0};
+#pragma omp parallel for schedule(dynamic, 1)
+    for (long long ri = 0; ri < (long long)nroots; ++ri) {
+        oracle::Sub s;
+        if (!oracle::decompose_root(pg, dpos, dseq, (uint32_t)ri, P, s, st)) continue;
+        auto sig = [](const oracle::Task& t) {
+            std::string x(t.lab.begin(), t.lab.end());
+            for (size_t i = 0; i < x.size(); ++i) if (x[i] == 5) x[i] = 3;   // H and U both mean "not in P, C, X"
+            return x;
+        };
+        std::vector<std::string> a, b;
+        uint64_t ta = 0, tb = 0;
+        oracle::ksearch(s, P, st, ta, [&](oracle::Task& t) { a.push_back(sig(t)); });
+        for (int d = 0; d <= s.n - s.hop; ++d)
+            oracle::ksearch(s, P, st, tb, [&](oracle::Task& t) { b.push_back(sig(t)); }, d);
+        std::sort(a.begin(), a.end());
+        std::sort(b.begin(), b.end());
+        if (a != b) bad++;
+    }
+    return bad;
+}
+
+// Decomposition only: per root rank, the local size n (0 if skipped/invalid) and |left|.
+long long oracle_root_sizes(const uint32_t* off, const uint32_t* adj, uint32_t n, int k, int q, int truss,
+                            uint32_t* out_n, uint32_t* out_left, uint64_t cap) {
+    oracle::Graph g = oracle::from_csr(off, adj, n), pg;
+    oracle::Params P{k, q, truss};
+    std::vector<int> dpos, dseq; std::vector<uint32_t> orig;
+    oracle::preprocess(g, P, pg, dpos, dseq, orig);
+    const long long lim = (long long)pg.n - q + 2;
+    const uint64_t nroots = lim > 0 ? (uint64_t)lim : 0;
+    oracle::Stats st;
+#pragma omp parallel for schedule(dynamic, 4)
+    for (long long ri = 0; ri < (long long)std::min<uint64_t>(nroots, cap); ++ri) {
+        oracle::Sub s;
+        // size-only pass: decompose_root rejects n > 1024 before building matrices
+        s.n = 0; s.nleft = 0;
+        oracle::decompose_root(pg, dpos, dseq, (uint32_t)ri, P, s, st);
+        out_n[ri] = (uint32_t)s.n;
+        out_left[ri] = (uint32_t)s.nleft;
+    }
+    return (long long)nroots;
+}
+
+// The reference's own k-search order: one sequential state machine per root.
+int oracle_enumerate_sequential(const uint32_t* off, const uint32_t* adj, uint32_t n, int k, int q, int truss,
+                                int threads, oracle_result* out) {
+    if (k < 2 || q < 1) return 1;
+    oracle::Graph g = oracle::from_csr(off, adj, n);
+    oracle::Params P{k, q, truss};
+    oracle::Result R = oracle::run(g, P, threads, 0, UINT64_MAX, 0, 1, true);
+    *out = oracle_result{R.count, R.hash, R.tasks, R.valid, R.truncated, R.depth_cap, R.too_big,
+                         R.pn, R.pm, R.max_n, R.max_left, R.ms_pre, R.ms_search};
+    return 0;
+}
+
 int oracle_enumerate_file(const char* path, int k, int q, int truss, int threads, oracle_result* out) {
     oracle::Graph g;
     int rc = oracle::load_bin(path, g);
@@ -837,6 +926,7 @@ long long oracle_preprocess(const uint32_t* off, const uint32_t* adj, uint32_t n
 int main(int argc, char** argv) {
     if (argc < 2) { fprintf(stderr, "usage: %s <graph.bin> -k K -q Q [-tr 0|1] [-threads N] [-roots B E]\n", argv[0]); return 1; }
     int k = 2, q = 8, tr = 0, th = 0;
+    bool seq = false;
     uint64_t rb = 0, re = UINT64_MAX;
     for (int i = 2; i < argc; ++i) {
         if (!strcmp(argv[i], "-k") && i + 1 < argc) k = atoi(argv[++i]);
@@ -844,11 +934,12 @@ int main(int argc, char** argv) {
         else if (!strcmp(argv[i], "-tr") && i + 1 < argc) tr = atoi(argv[++i]);
         else if (!strcmp(argv[i], "-threads") && i + 1 < argc) th = atoi(argv[++i]);
         else if (!strcmp(argv[i], "-roots") && i + 2 < argc) { rb = strtoull(argv[++i], 0, 10); re = strtoull(argv[++i], 0, 10); }
+        else if (!strcmp(argv[i], "-seq")) seq = true;
     }
     oracle::Graph g;
     if (oracle::load_bin(argv[1], g)) { fprintf(stderr, "cannot read %s\n", argv[1]); return 2; }
     oracle::Params P{k, q, tr};
-    oracle::Result R = oracle::run(g, P, th, rb, re);
+    oracle::Result R = oracle::run(g, P, th, rb, re, 0, 1, seq);
     printf("pn=%u pm=%u valid_roots=%llu max_n=%u max_left=%u truncated=%llu depth_capped=%llu oversized=%llu\n",
            R.pn, R.pm, (unsigned long long)R.valid, R.max_n, R.max_left, (unsigned long long)R.truncated,
            (unsigned long long)R.depth_cap, (unsigned long long)R.too_big);
