@@ -37,7 +37,10 @@ extern "C" {
 /* kplex_params.flags */
 #define KPLEX_FLAG_QUIET        0x1u  /* no stdout lines from the library */
 #define KPLEX_FLAG_NO_HASH      0x2u  /* skip the per-output hash (count only) */
-#define KPLEX_FLAG_FORCE_SPILL  0x4u  /* test hook: spill kSearch tasks to pinned host memory at every pause */
+#define KPLEX_FLAG_SPILL_HOST   0x4u  /* when the device task pool reaches thres * pool_slots, k-search writes
+                                         further tasks to pinned host memory (up to 4x the pool) instead of
+                                         pausing, and idle warps refill from there (north_star spill/refill;
+                                         the reference's spillToHost/reFillTasks are dead code, host:168-251) */
 #define KPLEX_FLAG_TEST_NO_WAIT 0x8u  /* test hook: branch warps give up every bounded wait at once, so the
                                          run must end with KPLEX_ERR_TIMEOUT instead of hanging */
 
@@ -67,7 +70,7 @@ typedef struct {
     uint32_t max_local_n;   /* largest root subgraph |{root} u C1 u C2| */
     uint32_t max_left;      /* largest root left set */
     uint32_t pauses;        /* kSearch pause/resume cycles */
-    uint32_t spilled;       /* task records moved to pinned host memory and back */
+    uint32_t spilled;       /* task records written to pinned host memory (KPLEX_FLAG_SPILL_HOST) */
     double ms_preprocess;   /* host core/truss/degeneracy */
     double ms_device;       /* device search: decomposition + k-search + branch-and-bound */
     double ms_ref_region;   /* preprocess + device search: the reference's "Total Time Elapsed" region */
@@ -145,6 +148,27 @@ long long kplex_preprocess_csr(const uint32_t* offsets, const uint32_t* neighbor
                                int k, int q, int truss, uint32_t omp_threads,
                                uint32_t* out_off, uint32_t* out_adj, int32_t* out_dpos, int32_t* out_dseq,
                                uint32_t* out_orig, uint64_t* out_m);
+
+/* Batched enumeration (no reference counterpart; the reference handles one
+ * graph per process).  Each job is an independent graph with its own k, q and
+ * truss setting; thres, flags, device and pool size come from `common`.  All
+ * jobs' roots are decomposed and searched together in one persistent launch,
+ * and per_job[i] receives job i's count, hash, valid roots, pn and pm
+ * (per_job may be NULL); *total receives the sums and timings.  Results are
+ * identical to separate kplex_enumerate_csr calls. */
+typedef struct {
+    const uint32_t* offsets;
+    const uint32_t* neighbors;
+    uint32_t n;
+    uint64_t m_directed;
+    int k, q, truss;
+} kplex_job;
+int kplex_enumerate_batch(const kplex_job* jobs, uint32_t njobs, const kplex_params* common,
+                          kplex_result* per_job, kplex_result* total);
+/* Two-stage batch: preprocess and upload once, then search (repeatable). */
+int kplex_prepare_batch(const kplex_job* jobs, uint32_t njobs, const kplex_params* common,
+                        kplex_prepared** h, kplex_result* total);
+int kplex_search_batch(kplex_prepared* h, kplex_result* per_job, kplex_result* total);
 
 const char* kplex_status_string(int status);
 /* Text of the last failure on the calling thread (CUDA message, parse error, ...). */

@@ -81,8 +81,6 @@ __global__ void __launch_bounds__(256) decompose_kernel(SearchParams sp) {
     const unsigned l = lane_id();
     const unsigned warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     DecompScratch S = decomp_scratch(sp, warp);
-    const int k = sp.k, q = sp.q;
-    const int lb2k = q - 2 * k, bd = q - k;
     __shared__ uint32_t s_alive_all[8][MAX_WORDS];
     __shared__ uint32_t s_row_all[8][2 * MAX_WORDS];
     uint32_t* s_alive = s_alive_all[threadIdx.x >> 5];
@@ -93,12 +91,28 @@ __global__ void __launch_bounds__(256) decompose_kernel(SearchParams sp) {
         if (l == 0) r = atomicAdd(&sp.ctr->decomp_next, 1u);
         r = __shfl_sync(FULL, r, 0);
         if (r >= sp.nroots) break;
+        // the root's graph: the last g with root_base <= r
+        uint32_t g = 0;
+        {
+            uint32_t lo = 0, hi = sp.ngraphs;
+            while (hi - lo > 1) { const uint32_t mid = (lo + hi) >> 1; if (sp.graphs[mid].root_base <= r) lo = mid; else hi = mid; }
+            g = lo;
+        }
+        const GraphInfo gi = sp.graphs[g];
+        const int k = gi.k, q = gi.q;
+        const int lb2k = q - 2 * k, bd = q - k;
         RootDesc desc{};
+        desc.graph = g;
+        desc.k = k;
+        desc.q = q;
         if (sp.shard_count > 1 && r % sp.shard_count != sp.shard_index) {   // another GPU's root
             if (l == 0) sp.roots[r] = desc;
             __syncwarp();
             continue;
         }
+        // loc/cnt are indexed by the graph's own vertex ids (vertex - vbase)
+        uint32_t* const loc = S.loc - gi.vbase;
+        uint32_t* const cnt = S.cnt - gi.vbase;
         const uint32_t root = (uint32_t)sp.dseq[r];
         const int pos = sp.dpos[root];
         desc.gid = root;
@@ -130,9 +144,9 @@ __global__ void __launch_bounds__(256) decompose_kernel(SearchParams sp) {
         if (nearlier > MAX_LOCAL) { nearlier = MAX_LOCAL; truncated = true; }
         __syncwarp();
         // loc: later j -> j (temporary), earlier -> EXCL until the left filter
-        for (int i = l; i < nlater; i += 32) S.loc[S.later[i]] = (uint32_t)i;
-        for (int i = l; i < nearlier; i += 32) S.loc[S.earlier[i]] = LOC_EXCL;
-        if (l == 0) S.loc[root] = LOC_EXCL;
+        for (int i = l; i < nlater; i += 32) loc[S.later[i]] = (uint32_t)i;
+        for (int i = l; i < nearlier; i += 32) loc[S.earlier[i]] = LOC_EXCL;
+        if (l == 0) loc[root] = LOC_EXCL;
         __syncwarp();
 
         // ---- C1 peel (src:142-180): synchronous rounds to the (q-2k) core of C1
@@ -154,7 +168,7 @@ __global__ void __launch_bounds__(256) decompose_kernel(SearchParams sp) {
                 int c = 0;
                 const uint32_t u = S.later[i];
                 for (uint32_t j = sp.off[u] + l; j < sp.off[u + 1]; j += 32) {
-                    const uint32_t x = S.loc[sp.adj[j]];
+                    const uint32_t x = loc[sp.adj[j]];
                     c += (x < (uint32_t)nlater) && test_bit(s_alive, x);
                 }
                 c = warp_sum(c);
@@ -189,21 +203,21 @@ __global__ void __launch_bounds__(256) decompose_kernel(SearchParams sp) {
             hop = 1 + cntc;
             if (l == 0) S.blk[0] = root;
             // later vertices: C1 members get local ids, peeled ones are excluded
-            for (int i = l; i < nlater; i += 32) S.loc[S.later[i]] = LOC_EXCL;
+            for (int i = l; i < nlater; i += 32) loc[S.later[i]] = LOC_EXCL;
             __syncwarp();
-            for (int i = 1 + l; i < hop; i += 32) S.loc[S.blk[i]] = (uint32_t)i;
-            if (l == 0) S.loc[root] = 0;
+            for (int i = 1 + l; i < hop; i += 32) loc[S.blk[i]] = (uint32_t)i;
+            if (l == 0) loc[root] = 0;
             __syncwarp();
 
             // ---- left filter (src:188-213): >= q-2k+1 neighbours in C1
             int nl1 = 0;
             for (int i = 0; i < nearlier; ++i) {
                 const uint32_t u = S.earlier[i];
-                const int c = count_local_nbrs(sp, S.loc, u, 1, (uint32_t)hop);
+                const int c = count_local_nbrs(sp, loc, u, 1, (uint32_t)hop);
                 if (c >= lb2k + 1) { if (l == 0) S.left[nl1] = u; ++nl1; }
             }
             __syncwarp();
-            for (int i = l; i < nl1; i += 32) S.loc[S.left[i]] = 1024u + (uint32_t)i;  // marks membership
+            for (int i = l; i < nl1; i += 32) loc[S.left[i]] = 1024u + (uint32_t)i;  // marks membership
             __syncwarp();
 
             // ---- 2-hop scan (src:217-273): count C1 neighbours of unvisited vertices
@@ -211,7 +225,7 @@ __global__ void __launch_bounds__(256) decompose_kernel(SearchParams sp) {
                 const uint32_t c1v = S.blk[i];
                 for (uint32_t j = sp.off[c1v] + l; j < sp.off[c1v + 1]; j += 32) {
                     const uint32_t w = sp.adj[j];
-                    if (S.loc[w] == LOC_NONE) atomicAdd(&S.cnt[w], 1u);
+                    if (loc[w] == LOC_NONE) atomicAdd(&cnt[w], 1u);
                 }
             }
             __syncwarp();
@@ -226,8 +240,8 @@ __global__ void __launch_bounds__(256) decompose_kernel(SearchParams sp) {
                     uint32_t w = 0;
                     if (j < sp.off[c1v + 1]) {
                         w = sp.adj[j];
-                        if (S.loc[w] == LOC_NONE) {
-                            const uint32_t c = atomicExch(&S.cnt[w], 0u);
+                        if (loc[w] == LOC_NONE) {
+                            const uint32_t c = atomicExch(&cnt[w], 0u);
                             if (c) {
                                 if (pos < sp.dpos[w]) takeC2 = (int)c >= lb2k + 2;
                                 else takeL = (int)c >= lb2k + 3;
@@ -256,8 +270,8 @@ __global__ void __launch_bounds__(256) decompose_kernel(SearchParams sp) {
         const bool valid = !skip && n >= q;
         if (valid && !oversized) {
             // final loc: blk -> local id, left -> 1024 + index
-            for (int i = l; i < n; i += 32) S.loc[S.blk[i]] = (uint32_t)i;
-            for (int i = l; i < nleft; i += 32) S.loc[S.left[i]] = 1024u + (uint32_t)i;
+            for (int i = l; i < n; i += 32) loc[S.blk[i]] = (uint32_t)i;
+            for (int i = l; i < nleft; i += 32) loc[S.left[i]] = 1024u + (uint32_t)i;
             __syncwarp();
             const uint32_t W = ((uint32_t)((n + 31) >> 5) + 3u) & ~3u;
             const uint32_t WL = nleft ? ((uint32_t)((nleft + 31) >> 5) + 3u) & ~3u : 0u;
@@ -285,7 +299,7 @@ __global__ void __launch_bounds__(256) decompose_kernel(SearchParams sp) {
                     __syncwarp();
                     const uint32_t u = S.blk[i];
                     for (uint32_t j = sp.off[u] + l; j < sp.off[u + 1]; j += 32) {
-                        const uint32_t x = S.loc[sp.adj[j]];
+                        const uint32_t x = loc[sp.adj[j]];
                         if (x < (uint32_t)n) atomicOr(&s_row[x >> 5], 1u << (x & 31));
                         else if (x >= 1024u && x < 1024u + (uint32_t)nleft) {
                             const uint32_t jl = x - 1024u;
@@ -347,6 +361,7 @@ __global__ void __launch_bounds__(256) decompose_kernel(SearchParams sp) {
                 desc.flags = ROOT_VALID;
                 if (l == 0) {
                     atomicAdd(&sp.ctr->valid_roots, 1u);
+                    atomicAdd(&sp.gvalid[g], 1u);
                     atomicMax(&sp.ctr->max_n, (unsigned)n);
                     atomicMax(&sp.ctr->max_left, (unsigned)nleft);
                     atomicMax(&sp.ctr->max_w, W);
@@ -361,6 +376,7 @@ __global__ void __launch_bounds__(256) decompose_kernel(SearchParams sp) {
             desc.flags = ROOT_VALID | ROOT_OVERSIZED;
             if (l == 0) {
                 atomicAdd(&sp.ctr->valid_roots, 1u);
+                atomicAdd(&sp.gvalid[g], 1u);
                 atomicAdd(&sp.ctr->oversized, 1u);
                 atomicMax(&sp.ctr->max_n, (unsigned)n);
                 atomicMax(&sp.ctr->max_left, (unsigned)nleft);
@@ -375,13 +391,13 @@ __global__ void __launch_bounds__(256) decompose_kernel(SearchParams sp) {
         }
         __syncwarp();
         // ---- restore scratch: loc for every id written, cnt already zeroed by exchange
-        for (int i = l; i < nlater; i += 32) S.loc[S.later[i]] = LOC_NONE;
-        for (int i = l; i < nearlier; i += 32) S.loc[S.earlier[i]] = LOC_NONE;
+        for (int i = l; i < nlater; i += 32) loc[S.later[i]] = LOC_NONE;
+        for (int i = l; i < nearlier; i += 32) loc[S.earlier[i]] = LOC_NONE;
         if (!skip && !oversized) {
-            for (int i = l; i < n; i += 32) S.loc[S.blk[i]] = LOC_NONE;
-            for (int i = l; i < nleft; i += 32) S.loc[S.left[i]] = LOC_NONE;
+            for (int i = l; i < n; i += 32) loc[S.blk[i]] = LOC_NONE;
+            for (int i = l; i < nleft; i += 32) loc[S.left[i]] = LOC_NONE;
         }
-        if (l == 0) S.loc[root] = LOC_NONE;
+        if (l == 0) loc[root] = LOC_NONE;
         __syncwarp();
         if (l == 0) sp.roots[r] = desc;
         __syncwarp();

@@ -38,8 +38,18 @@ enum : uint32_t {
 
 struct RootDesc {
     uint32_t n, hop, nleft, W;   // W: words per local row, multiple of 4
-    uint32_t WL, flags, gid, pad;
+    uint32_t WL, flags, gid, graph;
     uint64_t base;               // word offset of the root's block in the arena
+    int32_t k, q;                // the parameters of the root's graph
+};
+
+// One input graph of a search (a single-graph search has one).  Vertices of
+// graph g are [vbase, vbase + pn) in the concatenated pruned CSR; its roots are
+// [root_base, root_base + nroots).
+struct GraphInfo {
+    uint32_t vbase, pn, root_base, nroots;
+    int32_t k, q;
+    uint32_t pad[2];
 };
 
 struct TaskHdr {
@@ -75,6 +85,8 @@ struct Counters {
     unsigned int stuck_once;       // test hook: one pool slot claimed and never published
     unsigned long long stage_copies;  // adjacency matrices copied to shared memory
     unsigned long long ks_cycles;  // SM cycles producers spent in k-search
+    unsigned long long spilled;    // records written to the host spill ring
+    unsigned long long refilled;   // records read back from it
 };
 
 // Vyukov bounded MPMC ring: each slot carries a sequence number so that a
@@ -87,9 +99,8 @@ struct Pool {
 };
 
 struct SearchParams {
-    int k, q;
-    uint32_t nroots;           // number of root ranks considered
-    uint32_t pn;
+    uint32_t nroots;           // roots over all graphs
+    uint32_t pn;               // largest pruned vertex count of any graph (scratch sizing)
     const uint32_t* off;       // pruned CSR
     const uint32_t* adj;
     const int32_t* dpos;
@@ -103,6 +114,11 @@ struct SearchParams {
     uint32_t* pool_seq;        // per slot sequence (u64 position folded to 32 bits)
     uint32_t* pool_data;       // cap * slot_words
     uint32_t slot_words;       // 4 + 3 * Wt
+    Pool* spill_pool;          // spill ring: control + sequence words in HBM,
+    uint32_t* spill_seq;       // record data in mapped pinned host memory
+    uint32_t* spill_data;
+    uint32_t spill_on;
+    unsigned long long spill_pause_at;   // producers pause when the spill ring holds this many
     uint32_t Wt;               // words per bitset in a task record
     unsigned long long pause_at;   // k-search pauses when the pool holds this many records
     uint32_t* warp_scratch;    // decomposition per-warp scratch
@@ -115,6 +131,11 @@ struct SearchParams {
     uint32_t hash_on;
     uint32_t shard_index, shard_count;
     uint32_t test_stuck;       // test hook: the first push claims a slot and never publishes it
+    const GraphInfo* graphs;   // ngraphs entries
+    uint32_t ngraphs;
+    unsigned long long* gcount;   // per graph: maximal k-plexes
+    unsigned long long* ghash;    // per graph: hash sum
+    unsigned int* gvalid;         // per graph: valid roots
     uint32_t a_words;          // per-warp shared-memory copy of a root's A (0: read A from the arena)
     uint32_t stage_after;      // nodes on one root before its A is copied to shared memory
     const uint32_t* job_base;  // k-search jobs: root r owns jobs [job_base[r], job_base[r+1])

@@ -81,11 +81,28 @@ struct DevBuf {
     template <typename T> T* as() const { return static_cast<T*>(p); }
 };
 
+// Mapped pinned host memory (cudaHostAllocMapped), grown on demand.
+struct HostMappedBuf {
+    void* h = nullptr;
+    void* d = nullptr;
+    size_t bytes = 0;
+    int ensure(size_t want) {
+        if (want <= bytes && h) return KPLEX_OK;
+        if (h) { cudaFreeHost(h); h = d = nullptr; bytes = 0; }
+        cudaError_t e = cudaHostAlloc(&h, want, cudaHostAllocMapped | cudaHostAllocPortable);
+        if (e == cudaSuccess) e = cudaHostGetDevicePointer(&d, h, 0);
+        if (e != cudaSuccess) { cudaGetLastError(); h = d = nullptr; g_last_error = std::string("pinned host spill buffer: ") + cudaGetErrorString(e); return KPLEX_ERR_NOMEM; }
+        bytes = want;
+        return KPLEX_OK;
+    }
+};
+
 struct DeviceState {
     bool init = false;
     int sms = 0;
     cudaStream_t stream = nullptr;
-    DevBuf roots, ctr, scratch, arena, pool_seq, pool_data, pool, ks, stacks, jobs;
+    DevBuf roots, ctr, scratch, arena, pool_seq, pool_data, pool, ks, stacks, jobs, spill_ctl, spill_seq;
+    HostMappedBuf spill_data;
     Counters* h_ctr = nullptr;   // pinned
 };
 
@@ -121,22 +138,39 @@ static double ms_since(std::chrono::steady_clock::time_point t0) {
 
 using namespace kplex;
 
+// A set of preprocessed graphs resident on one device (one graph for
+// kplex_prepare, many for kplex_prepare_batch).  Graph g's pruned vertices are
+// [vbase, vbase + pn) of the concatenated CSR and its roots [root_base,
+// root_base + nroots) of the concatenated root order.
 struct kplex_prepared {
     int device = 0;
     kplex_params p{};
-    uint32_t pn = 0, pm = 0;
+    uint32_t ngraphs = 0;
+    uint32_t pn = 0, pm = 0, pn_max = 0, nroots = 0;
     double ms_pre = 0;
+    std::vector<GraphInfo> ginfo;
+    std::vector<uint32_t> gpm;
     uint32_t* d_off = nullptr;
     uint32_t* d_adj = nullptr;
     int32_t* d_dpos = nullptr;
     int32_t* d_dseq = nullptr;
     uint32_t* d_orig = nullptr;
+    GraphInfo* d_graphs = nullptr;
+    unsigned long long* d_gcount = nullptr;
+    unsigned long long* d_ghash = nullptr;
+    unsigned int* d_gvalid = nullptr;
 };
+
+static int check_kq(int k, int q) {
+    if (k < 2 || k > MAX_K - 1) { g_last_error = "k must be in [2, 31]"; return KPLEX_ERR_PARAM; }
+    if (q < 2 * k - 1) { g_last_error = "q must be >= 2k-1"; return KPLEX_ERR_PARAM; }
+    return KPLEX_OK;
+}
 
 static int check_params(const kplex_params* p) {
     if (!p) { g_last_error = "null params"; return KPLEX_ERR_PARAM; }
-    if (p->k < 2 || p->k > MAX_K - 1) { g_last_error = "k must be in [2, 31]"; return KPLEX_ERR_PARAM; }
-    if (p->q < 2 * p->k - 1) { g_last_error = "q must be >= 2k-1"; return KPLEX_ERR_PARAM; }
+    int rc = check_kq(p->k, p->q);
+    if (rc) return rc;
     if (!(p->thres > 0.0f) || p->thres > 1.0f) { g_last_error = "thres must be in (0, 1]"; return KPLEX_ERR_PARAM; }
     return KPLEX_OK;
 }
@@ -145,63 +179,123 @@ static void free_prepared(kplex_prepared* h) {
     if (!h) return;
     cudaSetDevice(h->device);
     cudaFree(h->d_off); cudaFree(h->d_adj); cudaFree(h->d_dpos); cudaFree(h->d_dseq); cudaFree(h->d_orig);
+    cudaFree(h->d_graphs); cudaFree(h->d_gcount); cudaFree(h->d_ghash); cudaFree(h->d_gvalid);
     delete h;
 }
 
-static int prepare_impl(const uint32_t* off, const uint32_t* adj, uint32_t n, uint64_t m, const kplex_params* p,
-                        kplex_prepared** out_h, kplex_result* out) {
-    int rc = check_params(p);
-    if (rc) return rc;
-    if (!off || (!adj && m) || (n && off[n] != m) || m > 0xffffffffull) { g_last_error = "inconsistent CSR"; return KPLEX_ERR_FORMAT; }
-    Csr g;
-    g.n = n;
-    g.off.assign(off, off + n + 1);
-    g.adj.assign(adj, adj + m);
-    std::string err;
-    rc = validate_csr(g, &err);
-    if (rc) { g_last_error = err; return rc; }
+struct HostJob {
+    const uint32_t* off;
+    const uint32_t* adj;
+    uint32_t n;
+    uint64_t m;
+    int k, q, truss;
+};
+
+// Validates, preprocesses (one host thread per graph when there are several)
+// and uploads a set of graphs.
+static int prepare_set(const std::vector<HostJob>& jobs, const kplex_params* p, kplex_prepared** out_h, kplex_result* out) {
+    if (!p || !(p->thres > 0.0f) || p->thres > 1.0f) { g_last_error = "thres must be in (0, 1]"; return KPLEX_ERR_PARAM; }
+    const size_t G = jobs.size();
+    for (const HostJob& j : jobs) {
+        int rc = check_kq(j.k, j.q);
+        if (rc) return rc;
+        if (!j.off || (!j.adj && j.m) || (j.n && j.off[j.n] != j.m) || j.m > 0xffffffffull) { g_last_error = "inconsistent CSR"; return KPLEX_ERR_FORMAT; }
+    }
     DeviceState* d = nullptr;
-    rc = device_state(p->device, &d);
+    int rc = device_state(p->device, &d);
     if (rc) return rc;
     auto t0 = std::chrono::steady_clock::now();
-    Prepped pre;
-    preprocess(g, p->k, p->q, p->truss, (int)p->omp_threads, pre);
+    std::vector<Prepped> pres(G);
+    std::vector<int> status(G, KPLEX_OK);
+    std::vector<std::string> errs(G);
+    auto one = [&](size_t g, int threads) {
+        const HostJob& j = jobs[g];
+        Csr c;
+        c.n = j.n;
+        c.off.assign(j.off, j.off + j.n + 1);
+        c.adj.assign(j.adj, j.adj + j.m);
+        status[g] = validate_csr(c, &errs[g]);
+        if (status[g] == KPLEX_OK) preprocess(c, j.k, j.q, j.truss, threads, pres[g]);
+    };
+    if (G == 1) one(0, (int)p->omp_threads);
+    else {
+#pragma omp parallel for schedule(dynamic, 1)
+        for (long long g = 0; g < (long long)G; ++g) one((size_t)g, 1);
+    }
+    for (size_t g = 0; g < G; ++g) if (status[g]) { g_last_error = errs[g]; return status[g]; }
     const double ms_pre = ms_since(t0);
-    if (!(p->flags & KPLEX_FLAG_QUIET)) printf("\npn = %u\n", pre.g.n);
+    if (G == 1 && !(p->flags & KPLEX_FLAG_QUIET)) printf("\npn = %u\n", pres[0].g.n);
+
     kplex_prepared* h = new kplex_prepared();
     h->device = p->device;
     h->p = *p;
-    h->pn = pre.g.n;
-    h->pm = pre.g.n ? pre.g.off[pre.g.n] : 0;
+    h->ngraphs = (uint32_t)G;
     h->ms_pre = ms_pre;
+    h->ginfo.resize(G);
+    h->gpm.resize(G);
+    uint64_t PN = 0, PM = 0, R = 0;
+    for (size_t g = 0; g < G; ++g) {
+        const Prepped& pr = pres[g];
+        const uint32_t pn = pr.g.n, pm = pn ? pr.g.off[pn] : 0;
+        const long long lim = (long long)pn - (long long)jobs[g].q + 2;   // src:44-45
+        const uint32_t nr = lim > 0 ? (uint32_t)std::min<long long>(lim, pn) : 0u;
+        h->ginfo[g] = GraphInfo{(uint32_t)PN, pn, (uint32_t)R, nr, jobs[g].k, jobs[g].q, {0, 0}};
+        h->gpm[g] = pm;
+        h->pn_max = std::max(h->pn_max, pn);
+        PN += pn; PM += pm; R += nr;
+    }
+    if (PN > 0x7fffffffull || PM > 0xffffffffull || R > 0x7fffffffull) { delete h; g_last_error = "batch too large"; return KPLEX_ERR_PARAM; }
+    h->pn = (uint32_t)PN; h->pm = (uint32_t)PM; h->nroots = (uint32_t)R;
+    std::vector<uint32_t> off(PN + 1), adj(std::max<uint64_t>(PM, 1)), orig(std::max<uint64_t>(PN, 1));
+    std::vector<int32_t> dpos(std::max<uint64_t>(PN, 1)), dseq(std::max<uint64_t>(R, 1));
+    uint64_t eb = 0;
+    for (size_t g = 0; g < G; ++g) {
+        const Prepped& pr = pres[g];
+        const GraphInfo& gi = h->ginfo[g];
+        for (uint32_t i = 0; i < gi.pn; ++i) {
+            off[gi.vbase + i] = (uint32_t)(eb + pr.g.off[i]);
+            dpos[gi.vbase + i] = pr.dpos[i];
+            orig[gi.vbase + i] = pr.orig[i];
+        }
+        for (uint32_t e = 0; e < h->gpm[g]; ++e) adj[eb + e] = gi.vbase + pr.g.adj[e];
+        for (uint32_t r = 0; r < gi.nroots; ++r) dseq[gi.root_base + r] = (int32_t)(gi.vbase + (uint32_t)pr.dseq[r]);
+        eb += h->gpm[g];
+    }
+    off[PN] = (uint32_t)PM;
     auto fail = [&](int code) { free_prepared(h); return code; };
-    const size_t pn = h->pn;
-    if (cudaMalloc(&h->d_off, (pn + 1) * 4) != cudaSuccess || cudaMalloc(&h->d_adj, std::max<size_t>(h->pm, 1) * 4) != cudaSuccess ||
-        cudaMalloc(&h->d_dpos, std::max<size_t>(pn, 1) * 4) != cudaSuccess || cudaMalloc(&h->d_dseq, std::max<size_t>(pn, 1) * 4) != cudaSuccess ||
-        cudaMalloc(&h->d_orig, std::max<size_t>(pn, 1) * 4) != cudaSuccess) {
-        cudaGetLastError(); g_last_error = "cudaMalloc for the pruned graph failed"; return fail(KPLEX_ERR_NOMEM);
+    if (cudaMalloc(&h->d_off, (PN + 1) * 4) != cudaSuccess || cudaMalloc(&h->d_adj, adj.size() * 4) != cudaSuccess ||
+        cudaMalloc(&h->d_dpos, dpos.size() * 4) != cudaSuccess || cudaMalloc(&h->d_dseq, dseq.size() * 4) != cudaSuccess ||
+        cudaMalloc(&h->d_orig, orig.size() * 4) != cudaSuccess || cudaMalloc(&h->d_graphs, G * sizeof(GraphInfo)) != cudaSuccess ||
+        cudaMalloc(&h->d_gcount, G * 8) != cudaSuccess || cudaMalloc(&h->d_ghash, G * 8) != cudaSuccess ||
+        cudaMalloc(&h->d_gvalid, G * 4) != cudaSuccess) {
+        cudaGetLastError(); g_last_error = "cudaMalloc for the pruned graphs failed"; return fail(KPLEX_ERR_NOMEM);
     }
-    if (!pre.g.off.empty()) CK(cudaMemcpyAsync(h->d_off, pre.g.off.data(), (pn + 1) * 4, cudaMemcpyHostToDevice, d->stream));
-    if (h->pm) CK(cudaMemcpyAsync(h->d_adj, pre.g.adj.data(), (size_t)h->pm * 4, cudaMemcpyHostToDevice, d->stream));
-    if (pn) {
-        CK(cudaMemcpyAsync(h->d_dpos, pre.dpos.data(), pn * 4, cudaMemcpyHostToDevice, d->stream));
-        CK(cudaMemcpyAsync(h->d_dseq, pre.dseq.data(), pn * 4, cudaMemcpyHostToDevice, d->stream));
-        CK(cudaMemcpyAsync(h->d_orig, pre.orig.data(), pn * 4, cudaMemcpyHostToDevice, d->stream));
-    }
+    CK(cudaMemcpyAsync(h->d_off, off.data(), off.size() * 4, cudaMemcpyHostToDevice, d->stream));
+    CK(cudaMemcpyAsync(h->d_adj, adj.data(), adj.size() * 4, cudaMemcpyHostToDevice, d->stream));
+    CK(cudaMemcpyAsync(h->d_dpos, dpos.data(), dpos.size() * 4, cudaMemcpyHostToDevice, d->stream));
+    CK(cudaMemcpyAsync(h->d_dseq, dseq.data(), dseq.size() * 4, cudaMemcpyHostToDevice, d->stream));
+    CK(cudaMemcpyAsync(h->d_orig, orig.data(), orig.size() * 4, cudaMemcpyHostToDevice, d->stream));
+    CK(cudaMemcpyAsync(h->d_graphs, h->ginfo.data(), G * sizeof(GraphInfo), cudaMemcpyHostToDevice, d->stream));
     CK(cudaStreamSynchronize(d->stream));
     if (out) { out->pn = h->pn; out->pm = h->pm; out->ms_preprocess = ms_pre; }
     *out_h = h;
     return KPLEX_OK;
 }
 
-static int search_impl(kplex_prepared* h, kplex_result* out) {
+static int prepare_impl(const uint32_t* off, const uint32_t* adj, uint32_t n, uint64_t m, const kplex_params* p,
+                        kplex_prepared** out_h, kplex_result* out) {
+    int rc = check_params(p);
+    if (rc) return rc;
+    return prepare_set({HostJob{off, adj, n, m, p->k, p->q, p->truss}}, p, out_h, out);
+}
+
+static int search_impl(kplex_prepared* h, kplex_result* out, kplex_result* per_graph = nullptr) {
     DeviceState* d = nullptr;
     int rc = device_state(h->device, &d);
     if (rc) return rc;
     const kplex_params& P = h->p;
     cudaStream_t st = d->stream;
-    const long long lim = (long long)h->pn - (long long)P.q + 2;   // src:44-45
-    const uint32_t nroots = lim > 0 ? (uint32_t)std::min<long long>(lim, h->pn) : 0u;
+    const uint32_t nroots = h->nroots;
     uint32_t launches = 0;
     cudaEvent_t e0, e1, ka, kb;
     CK(cudaEventCreate(&e0));
@@ -223,8 +317,10 @@ static int search_impl(kplex_prepared* h, kplex_result* out) {
     };
 
     SearchParams sp{};
-    sp.k = P.k; sp.q = P.q; sp.nroots = nroots; sp.pn = h->pn;
+    sp.nroots = nroots; sp.pn = h->pn_max;
     sp.off = h->d_off; sp.adj = h->d_adj; sp.dpos = h->d_dpos; sp.dseq = h->d_dseq; sp.orig = h->d_orig;
+    sp.graphs = h->d_graphs; sp.ngraphs = h->ngraphs;
+    sp.gcount = h->d_gcount; sp.ghash = h->d_ghash; sp.gvalid = h->d_gvalid;
     sp.hash_on = (P.flags & KPLEX_FLAG_NO_HASH) ? 0u : 1u;
     sp.shard_index = P.shard_count > 1 ? P.shard_index : 0u;
     sp.shard_count = P.shard_count > 1 ? P.shard_count : 1u;
@@ -237,7 +333,7 @@ static int search_impl(kplex_prepared* h, kplex_result* out) {
 
     // ---------------- decomposition (with arena growth on overflow)
     const uint32_t dec_warps = std::max<uint32_t>(8, std::min<uint32_t>((uint32_t)d->sms * 16, ((nroots + 7) / 8) * 8));
-    sp.scratch_words = decomp_scratch_words_host(h->pn);
+    sp.scratch_words = decomp_scratch_words_host(h->pn_max);
     if ((rc = d->scratch.ensure((size_t)dec_warps * sp.scratch_words * 4))) return rc;
     sp.warp_scratch = d->scratch.as<uint32_t>();
     size_t arena_words = std::max<size_t>(d->arena.bytes / 4, (size_t)1 << 22);
@@ -247,8 +343,11 @@ static int search_impl(kplex_prepared* h, kplex_result* out) {
         sp.arena = d->arena.as<uint32_t>();
         sp.arena_cap = arena_words;
         CK(cudaMemsetAsync(sp.ctr, 0, sizeof(Counters), st));
+        CK(cudaMemsetAsync(sp.gcount, 0, (size_t)h->ngraphs * 8, st));
+        CK(cudaMemsetAsync(sp.ghash, 0, (size_t)h->ngraphs * 8, st));
+        CK(cudaMemsetAsync(sp.gvalid, 0, (size_t)h->ngraphs * 4, st));
         if (nroots) {
-            init_decomp_scratch<<<d->sms * 4, 256, 0, st>>>(sp.warp_scratch, sp.scratch_words, h->pn, dec_warps);
+            init_decomp_scratch<<<d->sms * 4, 256, 0, st>>>(sp.warp_scratch, sp.scratch_words, h->pn_max, dec_warps);
             if ((rc = timed([&] { decompose_kernel<<<dec_warps / 8, 256, 0, st>>>(sp); }, ms_dec))) return rc;
             launches += 2;
         }
@@ -292,7 +391,7 @@ static int search_impl(kplex_prepared* h, kplex_result* out) {
     // tuning knobs (environment): blocks per SM the kernel is compiled for (2 or 3) and
     // how many nodes a warp processes on one root before copying its A to shared memory
     const char* eb = getenv("KPLEX_BLOCKS_PER_SM");
-    const int minb = (eb && atoi(eb) == 2) ? 2 : 3;
+    const int minb = (eb && atoi(eb) == 3) ? 3 : 2;   // measured: 2 blocks x 128 registers beats 3 x 80 + spills
     const char* es = getenv("KPLEX_STAGE_AFTER");
     sp.stage_after = es ? (uint32_t)atoi(es) : 8u;
     auto kfn = minb == 2 ? search_kernel_2 : search_kernel_3;
@@ -318,6 +417,20 @@ static int search_impl(kplex_prepared* h, kplex_result* out) {
     sp.pause_at = (unsigned long long)std::max<long long>(pause, 1);
     if ((rc = d->stacks.ensure((size_t)nwarps * sp.stack_depth * sp.slot_words * 4))) return rc;
     sp.stacks = d->stacks.as<uint32_t>();
+    if (P.flags & KPLEX_FLAG_SPILL_HOST) {
+        // spill ring: control and sequence words in HBM, records in mapped pinned host memory
+        const unsigned long long scap = std::min<unsigned long long>(4 * cap, 1ull << 24);
+        if ((rc = d->spill_ctl.ensure(sizeof(Pool)))) return rc;
+        if ((rc = d->spill_seq.ensure((size_t)scap * 4))) return rc;
+        if ((rc = d->spill_data.ensure((size_t)scap * sp.slot_words * 4))) return rc;
+        sp.spill_pool = d->spill_ctl.as<Pool>();
+        sp.spill_seq = d->spill_seq.as<uint32_t>();
+        sp.spill_data = static_cast<uint32_t*>(d->spill_data.d);
+        sp.spill_on = 1;
+        sp.spill_pause_at = scap > blocks ? scap - blocks : 1;
+        init_pool<<<d->sms * 4, 256, 0, st>>>(sp.spill_seq, scap, sp.spill_pool);
+        ++launches;
+    }
     if (P.flags & KPLEX_FLAG_TEST_NO_WAIT) {   // failure-detection test hook
         sp.test_stuck = 1;
         sp.spin_limit = 1u << 14;
@@ -341,6 +454,21 @@ static int search_impl(kplex_prepared* h, kplex_result* out) {
     cudaEventDestroy(kb);
     const uint32_t pauses = hc.ks_paused;
     if (!hc.error && hp.head != hp.tail) { hc.error = KPLEX_ERR_TIMEOUT; g_last_error = "branch warps gave up with records left in the pool"; }
+    if (per_graph) {
+        const size_t G = h->ngraphs;
+        std::vector<unsigned long long> gc(G), gh(G);
+        std::vector<unsigned int> gv(G);
+        CK(cudaMemcpy(gc.data(), sp.gcount, G * 8, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(gh.data(), sp.ghash, G * 8, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(gv.data(), sp.gvalid, G * 4, cudaMemcpyDeviceToHost));
+        for (size_t g = 0; g < G; ++g) {
+            kplex_result& r = per_graph[g];
+            memset(&r, 0, sizeof r);
+            r.count = gc[g]; r.hash = gh[g]; r.valid_roots = gv[g];
+            r.pn = h->ginfo[g].pn; r.pm = h->gpm[g];
+            r.status = (int)hc.error;
+        }
+    }
     if (out) {
         out->count = hc.count;
         out->hash = hc.hash;
@@ -352,7 +480,7 @@ static int search_impl(kplex_prepared* h, kplex_result* out) {
         out->max_local_n = hc.max_n;
         out->max_left = hc.max_left;
         out->pauses = pauses;
-        out->spilled = 0;
+        out->spilled = (uint32_t)std::min<unsigned long long>(hc.spilled, 0xffffffffull);
         out->ms_preprocess = h->ms_pre;
         out->ms_device = ms;
         out->ms_ref_region = h->ms_pre + ms;
@@ -528,6 +656,52 @@ int kplex_enumerate_csr(const uint32_t* offsets, const uint32_t* neighbors, uint
         printf("Total tasks generated: %u\n", (unsigned)(r->tasks & 0xffffffffu));
         printf("\nKernel Launch Successfully\n");
     }
+    return rc;
+}
+
+int kplex_prepare_batch(const kplex_job* jobs, uint32_t njobs, const kplex_params* common, kplex_prepared** h,
+                        kplex_result* total) {
+    if (!h || !common || (!jobs && njobs)) return KPLEX_ERR_PARAM;
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (total) memset(total, 0, sizeof(*total));
+    if (njobs == 0) { g_last_error = "empty batch"; return KPLEX_ERR_PARAM; }
+    std::vector<HostJob> hj(njobs);
+    for (uint32_t i = 0; i < njobs; ++i)
+        hj[i] = HostJob{jobs[i].offsets, jobs[i].neighbors, jobs[i].n, jobs[i].m_directed, jobs[i].k, jobs[i].q, jobs[i].truss};
+    kplex_params p = *common;
+    p.flags |= KPLEX_FLAG_QUIET;
+    int rc = prepare_set(hj, &p, h, total);
+    if (total) total->status = rc;
+    return rc;
+}
+
+int kplex_search_batch(kplex_prepared* h, kplex_result* per_job, kplex_result* total) {
+    if (!h) return KPLEX_ERR_PARAM;
+    std::lock_guard<std::mutex> lk(g_mu);
+    auto t0 = std::chrono::steady_clock::now();
+    kplex_result tmp;
+    kplex_result* r = total ? total : &tmp;
+    memset(r, 0, sizeof(*r));
+    int rc = search_impl(h, r, per_job);
+    r->status = rc;
+    r->ms_total = ms_since(t0);
+    return rc;
+}
+
+int kplex_enumerate_batch(const kplex_job* jobs, uint32_t njobs, const kplex_params* common, kplex_result* per_job,
+                          kplex_result* total) {
+    auto t0 = std::chrono::steady_clock::now();
+    kplex_prepared* h = nullptr;
+    kplex_result tmp;
+    kplex_result* r = total ? total : &tmp;
+    int rc = kplex_prepare_batch(jobs, njobs, common, &h, r);
+    if (rc) return rc;
+    const double ms_pre = r->ms_preprocess;
+    rc = kplex_search_batch(h, per_job, r);
+    r->ms_preprocess = ms_pre;
+    r->ms_ref_region = ms_pre + r->ms_device;
+    kplex_release(h);
+    r->ms_total = ms_since(t0);
     return rc;
 }
 

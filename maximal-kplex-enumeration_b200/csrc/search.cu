@@ -28,7 +28,8 @@ namespace kplex {
 
 // ============================================================== root view
 struct RootView {
-    uint32_t n, hop, nleft, W, WL;
+    uint32_t n, hop, nleft, W, WL, graph;
+    int k, q;
     const uint32_t* A;
     const uint32_t* M2;
     const uint32_t* M4;
@@ -42,6 +43,7 @@ __device__ __forceinline__ RootView root_view(const SearchParams& sp, uint32_t r
     const RootDesc d = sp.roots[r];
     RootView v;
     v.n = d.n; v.hop = d.hop; v.nleft = d.nleft; v.W = d.W; v.WL = d.WL;
+    v.graph = d.graph; v.k = d.k; v.q = d.q;
     const uint32_t* A = sp.arena + d.base;
     v.A = A;
     v.M2 = A + (uint64_t)d.n * d.W;
@@ -141,7 +143,7 @@ __device__ void ks_start(const SearchParams& sp, const KsSlot& S, uint32_t r, ui
         S.nc2() = keep;
         S.sz() = 1;
         S.w[4] = d;   // chain depth: the frame's depth in the reference's stack
-        S.fr()[0] = fr_pack((uint32_t)(sp.k - 1), 1, d < m ? 2u : 0u, 0);
+        S.fr()[0] = fr_pack((uint32_t)(rd.k - 1), 1, d < m ? 2u : 0u, 0);
         S.root() = r;
     }
     __syncwarp();
@@ -155,7 +157,7 @@ __device__ bool ks_upper_bound(const SearchParams& sp, const RootView& R, const 
     bool ok = true;
     for (uint32_t i = l; i < np; i += 32) {
         const uint32_t u = S.P()[i];
-        if (row_and_popc(R.A + (uint64_t)u * R.W, S.mask(), R.W) + sp.k < sp.q) ok = false;
+        if (row_and_popc(R.A + (uint64_t)u * R.W, S.mask(), R.W) + R.k < R.q) ok = false;
     }
     ok = __all_sync(FULL, ok);
     __syncwarp();
@@ -173,9 +175,9 @@ struct Emitted {
 // saved state resumes exactly where the reference resumes after its pause.
 __device__ int ks_advance(const SearchParams& sp, const KsSlot& S, Emitted* e) {
     const unsigned l = lane_id();
-    const int k = sp.k, q = sp.q;
     const uint32_t r = S.root();
     const RootView R = root_view(sp, r);
+    const int k = R.k, q = R.q;
     const uint32_t n = R.n, W = R.W;
     uint32_t C1w = S.bits()[l], Xw = S.bits()[MAX_WORDS + l], Pw = S.bits()[2 * MAX_WORDS + l];
     uint32_t sz = S.sz(), np = S.np(), nc2 = S.nc2();
@@ -435,7 +437,7 @@ __device__ __forceinline__ void pivot_tree(int& m, int& v, int& p, int& idx) {
 __device__ bool left_maximal(const SearchParams& sp, const RootView& R, const BnbSmem& m, int s, const uint16_t* deg,
                              const uint32_t* sS, unsigned long long& bb) {
     const unsigned l = lane_id();
-    const int k = sp.k;
+    const int k = R.k;
     if (R.nleft == 0) return true;
     const uint32_t WL = R.WL, W = R.W;
     uint32_t lc = 0;
@@ -520,7 +522,7 @@ struct WarpWork {
 // on the warp's stack.
 __device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootView& R, const uint32_t* A, Node* t, WarpWork& ww) {
     const unsigned l = lane_id();
-    const int k = sp.k, q = sp.q;
+    const int k = R.k, q = R.q;
     const uint32_t W = R.W, Wt = sp.Wt, SW = sp.slot_words;
     const uint32_t np = t->np, nc = t->nc, nx = t->nx;
     const uint32_t Pw = t->Pw, Cw = t->Cw, Xw = t->Xw;
@@ -711,7 +713,9 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
     const BnbSmem m = bnb_smem(smem + KL.total + wib * bnb_smem_words(nmax, SW, sp.a_words), nmax, SW);
     const uint32_t* A = nullptr;
     uint32_t same_root = 0;
-    unsigned long long stage_copies = 0, ks_cycles = 0;
+    uint32_t acc_graph = 0;
+    unsigned long long tot_cnt = 0, tot_hsum = 0;
+    unsigned long long stage_copies = 0, ks_cycles = 0, spilled = 0, refilled = 0;
     WarpWork ww;
     ww.stack = sp.stacks + (uint64_t)warp * sp.stack_depth * SW;
     ww.sbot = ww.stop = 0;
@@ -746,6 +750,12 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
             if (t.root != cur_root) {
                 R = root_view(sp, t.root);
                 cur_root = t.root;
+                if (R.graph != acc_graph) {   // results are kept per input graph
+                    if (l == 0 && (ww.cnt || ww.hsum)) { atomicAdd(&sp.gcount[acc_graph], ww.cnt); atomicAdd(&sp.ghash[acc_graph], ww.hsum); }
+                    tot_cnt += ww.cnt; tot_hsum += ww.hsum;
+                    ww.cnt = ww.hsum = 0;
+                    acc_graph = R.graph;
+                }
                 A = R.A;
                 same_root = 0;
             } else if (++same_root == sp.stage_after && R.n * R.W <= sp.a_words) {
@@ -769,8 +779,15 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
         // ---------------- producer: k-search
         if (producer) {
             const unsigned long long ps = pool_size_warp(sp);
+            // with spilling on, a full-enough pool sends new tasks to host memory
+            // instead of pausing, until the spill ring itself is at its threshold
+            int to_host = 0;
+            if (sp.spill_on && ps >= sp.pause_at) {
+                if (l == 0) to_host = ring_size(spill_ring(sp)) < sp.spill_pause_at;
+                to_host = __shfl_sync(FULL, to_host, 0);
+            }
             if (paused && ps < resume_at) paused = false;
-            if (!paused && ps >= sp.pause_at) {
+            if (!paused && ps >= sp.pause_at && !to_host) {
                 paused = true;
                 if (l == 0) atomicAdd(&sp.ctr->ks_paused, 1u);
             }
@@ -805,14 +822,20 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
                         // stage this lane's words in shared memory; the record is hdr | P | C | X
                         m.P[l] = e.Pw; m.NC[l] = e.Cw; m.NX[l] = e.Xw;
                         __syncwarp();
-                        const bool pushed = pool_push(sp, [&](unsigned i) -> uint32_t {
+                        auto word = [&](unsigned i) -> uint32_t {
                             if (i == 0) return r;
                             if (i == 1) return e.np | (e.nc << 16);
                             if (i == 2) return e.nx;
                             if (i < 4) return 0u;
                             const unsigned j = i - 4, which = j / Wt, wi = j % Wt;
                             return which == 0 ? m.P[wi] : (which == 1 ? m.NC[wi] : m.NX[wi]);
-                        });
+                        };
+                        bool pushed = false;
+                        if (to_host) {   // spill: the record goes to pinned host memory
+                            pushed = ring_push(sp, spill_ring(sp), word);
+                            if (pushed) ++spilled;
+                        }
+                        if (!pushed) pushed = pool_push(sp, word);
                         if (!pushed) {   // ring full: keep the task
                             t.root = r; t.np = e.np; t.nc = e.nc; t.nx = e.nx;
                             t.Pw = e.Pw; t.Cw = e.Cw; t.Xw = e.Xw;
@@ -830,15 +853,17 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
                 }
             }
         }
-        // ---------------- consumer: take a record from the pool
+        // ---------------- consumer: take a record from the pool, else refill from the spill ring
         {
-            int nonempty = 0;
-            if (l == 0) nonempty = pool_size(sp) > 0;
-            nonempty = __shfl_sync(FULL, nonempty, 0);
-            if (nonempty) {
+            int which = 0;   // 1: main pool, 2: spill ring
+            if (l == 0) which = pool_size(sp) > 0 ? 1 : (spill_size(sp) > 0 ? 2 : 0);
+            which = __shfl_sync(FULL, which, 0);
+            if (which) {
                 if (l == 0) atomicAdd(&sp.ctr->busy, 1u);
                 __syncwarp();
-                if (pool_pop(sp, m.rec)) {
+                const bool got = which == 1 ? pool_pop(sp, m.rec) : ring_pop(sp, spill_ring(sp), m.rec);
+                if (got) {
+                    if (which == 2) ++refilled;
                     load_record(m.rec, Wt, &t, false);
                     have = true;
                     counted = true;
@@ -856,7 +881,7 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
             __threadfence();
             const unsigned nr = *(volatile unsigned*)&sp.ctr->next_root;
             const unsigned live = *(volatile unsigned*)&sp.ctr->ks_active;
-            const unsigned long long ps = pool_size(sp);
+            const unsigned long long ps = pool_size(sp) + spill_size(sp);
             const unsigned b = *(volatile unsigned*)&sp.ctr->busy;
             done = nr >= sp.njobs && live == 0 && ps == 0 && b == 0;
         }
@@ -871,8 +896,9 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
         __nanosleep(idle < 64 ? 100 : 1000);
     }
     if (l == 0) {
-        atomicAdd(&sp.ctr->count, ww.cnt);
-        atomicAdd(&sp.ctr->hash, ww.hsum);
+        if (ww.cnt || ww.hsum) { atomicAdd(&sp.gcount[acc_graph], ww.cnt); atomicAdd(&sp.ghash[acc_graph], ww.hsum); }
+        atomicAdd(&sp.ctr->count, tot_cnt + ww.cnt);
+        atomicAdd(&sp.ctr->hash, tot_hsum + ww.hsum);
         atomicAdd(&sp.ctr->tasks, ww.tasks + ks_tasks);
         atomicAdd(&sp.ctr->ks_tasks, ks_tasks);
         atomicAdd(&sp.ctr->nodes, ww.nodes);
@@ -880,6 +906,8 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
         atomicAdd(&sp.ctr->bnb_done, 1u);
         atomicAdd(&sp.ctr->stage_copies, stage_copies);
         atomicAdd(&sp.ctr->ks_cycles, ks_cycles);
+        atomicAdd(&sp.ctr->spilled, spilled);
+        atomicAdd(&sp.ctr->refilled, refilled);
     }
 }
 

@@ -66,12 +66,27 @@ __device__ __forceinline__ int row_and_popc(const uint32_t* __restrict__ row, co
 }
 
 // ---------------------------------------------------------------- task pool
-// Enqueue one record (slot_words words, lane l supplies words l, l+32, ...
+// A ring is a control block (head, tail, cap) and one sequence word per slot in
+// device memory, plus the record data.  The data of the main pool is in HBM;
+// the spill ring keeps its data in mapped pinned host memory, so only plain
+// loads and stores cross the bus (no GPU atomics on host memory) and a
+// system-scope fence orders them before the sequence word is published.
+struct Ring {
+    Pool* ctl;
+    uint32_t* seq;
+    uint32_t* data;
+    int sys;   // data lives in host memory
+};
+
+__device__ __forceinline__ Ring main_ring(const SearchParams& sp) { return Ring{sp.pool, sp.pool_seq, sp.pool_data, 0}; }
+__device__ __forceinline__ Ring spill_ring(const SearchParams& sp) { return Ring{sp.spill_pool, sp.spill_seq, sp.spill_data, 1}; }
+
+// Enqueue one record (slot_words words; lane l supplies words l, l+32, ...
 // through `word(i)`).  Returns false when the ring is full or the bounded
 // retry loop gives up; the caller keeps the record.
 template <typename WordFn>
-__device__ inline bool pool_push(const SearchParams& sp, WordFn word) {
-    Pool* pool = sp.pool;
+__device__ inline bool ring_push(const SearchParams& sp, const Ring& r, WordFn word) {
+    Pool* pool = r.ctl;
     const unsigned l = lane_id();
     unsigned long long pos = 0;
     int ok = 0;
@@ -79,7 +94,7 @@ __device__ inline bool pool_push(const SearchParams& sp, WordFn word) {
         const unsigned long long cap = pool->cap;
         for (unsigned long long it = 0; it < sp.spin_limit; ++it) {
             pos = atomicAdd(&pool->tail, 0ull);
-            const uint32_t seq = atomicAdd(&sp.pool_seq[pos % cap], 0u);
+            const uint32_t seq = atomicAdd(&r.seq[pos % cap], 0u);
             const int dif = (int)(seq - (uint32_t)pos);
             if (dif == 0) {
                 if (atomicCAS(&pool->tail, pos, pos + 1) == pos) { ok = 1; break; }
@@ -97,18 +112,18 @@ __device__ inline bool pool_push(const SearchParams& sp, WordFn word) {
         if (__shfl_sync(FULL, stuck, 0)) return true;
     }
     const unsigned long long slot = pos % pool->cap;
-    uint32_t* dst = sp.pool_data + slot * sp.slot_words;
+    uint32_t* dst = r.data + slot * sp.slot_words;
     for (unsigned i = l; i < sp.slot_words; i += 32) __stcg(dst + i, word(i));
-    __threadfence();
+    if (r.sys) __threadfence_system(); else __threadfence();
     __syncwarp();
-    if (l == 0) atomicExch(&sp.pool_seq[slot], (uint32_t)(pos + 1));
+    if (l == 0) atomicExch(&r.seq[slot], (uint32_t)(pos + 1));
     return true;
 }
 
-// Dequeue one record into dst (smem or gmem, slot_words words).  Returns
-// false if the ring looks empty (a record still being published counts as empty).
-__device__ inline bool pool_pop(const SearchParams& sp, uint32_t* dst) {
-    Pool* pool = sp.pool;
+// Dequeue one record into dst (slot_words words).  Returns false if the ring
+// looks empty (a record still being published counts as empty).
+__device__ inline bool ring_pop(const SearchParams& sp, const Ring& r, uint32_t* dst) {
+    Pool* pool = r.ctl;
     const unsigned l = lane_id();
     unsigned long long pos = 0;
     int ok = 0;
@@ -116,7 +131,7 @@ __device__ inline bool pool_pop(const SearchParams& sp, uint32_t* dst) {
         const unsigned long long cap = pool->cap;
         for (unsigned long long it = 0; it < sp.spin_limit; ++it) {
             pos = atomicAdd(&pool->head, 0ull);
-            const uint32_t seq = atomicAdd(&sp.pool_seq[pos % cap], 0u);
+            const uint32_t seq = atomicAdd(&r.seq[pos % cap], 0u);
             const int dif = (int)(seq - (uint32_t)(pos + 1));
             if (dif == 0) {
                 if (atomicCAS(&pool->head, pos, pos + 1) == pos) { ok = 1; break; }
@@ -131,19 +146,25 @@ __device__ inline bool pool_pop(const SearchParams& sp, uint32_t* dst) {
     const unsigned long long cap = pool->cap;
     const unsigned long long slot = pos % cap;
     __threadfence();
-    const uint32_t* src = sp.pool_data + slot * sp.slot_words;
+    const uint32_t* src = r.data + slot * sp.slot_words;
     for (unsigned i = l; i < sp.slot_words; i += 32) dst[i] = __ldcg(src + i);
     __threadfence();
     __syncwarp();
-    if (l == 0) atomicExch(&sp.pool_seq[slot], (uint32_t)(pos + cap));
+    if (l == 0) atomicExch(&r.seq[slot], (uint32_t)(pos + cap));
     return true;
 }
 
-__device__ __forceinline__ unsigned long long pool_size(const SearchParams& sp) {
-    const unsigned long long t = *(volatile unsigned long long*)&sp.pool->tail;
-    const unsigned long long h = *(volatile unsigned long long*)&sp.pool->head;
+__device__ __forceinline__ unsigned long long ring_size(const Ring& r) {
+    const unsigned long long t = *(volatile unsigned long long*)&r.ctl->tail;
+    const unsigned long long h = *(volatile unsigned long long*)&r.ctl->head;
     return t > h ? t - h : 0ull;
 }
+
+template <typename WordFn>
+__device__ inline bool pool_push(const SearchParams& sp, WordFn word) { return ring_push(sp, main_ring(sp), word); }
+__device__ inline bool pool_pop(const SearchParams& sp, uint32_t* dst) { return ring_pop(sp, main_ring(sp), dst); }
+__device__ __forceinline__ unsigned long long pool_size(const SearchParams& sp) { return ring_size(main_ring(sp)); }
+__device__ __forceinline__ unsigned long long spill_size(const SearchParams& sp) { return sp.spill_on ? ring_size(spill_ring(sp)) : 0ull; }
 
 // pool_size read once by lane 0 and broadcast, so every lane takes the same branch
 __device__ __forceinline__ unsigned long long pool_size_warp(const SearchParams& sp) {

@@ -19,7 +19,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libkplex.so")
 
 OK, ERR_PARAM, ERR_IO, ERR_FORMAT, ERR_CUDA, ERR_NOMEM, ERR_CAPACITY, ERR_TIMEOUT, ERR_NO_DEVICE, ERR_INTERNAL = range(10)
-FLAG_QUIET, FLAG_NO_HASH, FLAG_FORCE_SPILL, FLAG_TEST_NO_WAIT = 0x1, 0x2, 0x4, 0x8
+FLAG_QUIET, FLAG_NO_HASH, FLAG_SPILL_HOST, FLAG_TEST_NO_WAIT = 0x1, 0x2, 0x4, 0x8
 
 
 class KplexError(RuntimeError):
@@ -51,6 +51,12 @@ class Result(ctypes.Structure):
 class Graph(ctypes.Structure):
     _fields_ = [("n", ctypes.c_uint32), ("m_directed", ctypes.c_uint64),
                 ("offsets", ctypes.POINTER(ctypes.c_uint32)), ("neighbors", ctypes.POINTER(ctypes.c_uint32))]
+
+
+class Job(ctypes.Structure):
+    _fields_ = [("offsets", ctypes.POINTER(ctypes.c_uint32)), ("neighbors", ctypes.POINTER(ctypes.c_uint32)),
+                ("n", ctypes.c_uint32), ("m_directed", ctypes.c_uint64), ("k", ctypes.c_int), ("q", ctypes.c_int),
+                ("truss", ctypes.c_int)]
 
 
 class GenSpec(ctypes.Structure):
@@ -103,6 +109,11 @@ def lib() -> ctypes.CDLL:
                                            ctypes.c_int, ctypes.c_uint32, u32p, u32p, i32p, i32p, u32p,
                                            ctypes.POINTER(ctypes.c_uint64)]
         L.kplex_preprocess_csr.restype = ctypes.c_longlong
+        L.kplex_enumerate_batch.argtypes = [ctypes.POINTER(Job), ctypes.c_uint32, ctypes.POINTER(Params),
+                                            ctypes.POINTER(Result), ctypes.POINTER(Result)]
+        L.kplex_prepare_batch.argtypes = [ctypes.POINTER(Job), ctypes.c_uint32, ctypes.POINTER(Params),
+                                          ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(Result)]
+        L.kplex_search_batch.argtypes = [ctypes.c_void_p, ctypes.POINTER(Result), ctypes.POINTER(Result)]
         _lib = L
     return _lib
 
@@ -240,6 +251,84 @@ def preprocess(off: np.ndarray, adj: np.ndarray, k: int, q: int, truss: int = 0,
         raise _err(int(-pn))
     return {"pn": int(pn), "off": o_off[: pn + 1], "adj": o_adj[: m.value], "dpos": o_dpos[:pn], "dseq": o_dseq[:pn],
             "orig": o_orig[:pn]}
+
+
+def batch_workload(count: int = 4096, seed: int = 4):
+    """The batched workload: `count` independent seeded graphs.  Per graph: n log-uniform
+    in [64, 2048], Chung-Lu mean degree U[8, 24] with exponent 2.3, 1-8 planted groups
+    of 10-30 vertices at density U[0.85, 0.95], k uniform in {2, 3, 4}, q uniform in [8, 20].
+    Returns a list of (offsets, neighbors, k, q)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        n = int(round(float(np.exp(rng.uniform(np.log(64), np.log(2048))))))
+        deg = float(rng.uniform(8, 24))
+        groups = min(int(rng.integers(1, 9)), max(1, n // 30))   # groups never exceed the graph
+        gmax = int(min(30, n // groups))
+        spec = dict(seed=int(seed) * 1_000_003 + i, n=n, base_edges=int(round(n * deg / 2)), exponent=2.3,
+                    max_degree=0, groups=groups, group_min=min(10, gmax), group_max=gmax,
+                    density_min=0.85, density_max=0.95)
+        off, adj = generate(spec)
+        k = int(rng.integers(2, 5))
+        q = int(rng.integers(8, 21))
+        out.append((off, adj, k, q))
+    return out
+
+
+class PreparedBatch:
+    """A batch of graphs resident on the device; search() reruns the device stage."""
+
+    def __init__(self, handle, n, total):
+        self.handle, self.n, self.pre = handle, n, total
+
+    def search(self):
+        per = (Result * self.n)()
+        tot = Result()
+        rc = lib().kplex_search_batch(self.handle, per, ctypes.byref(tot))
+        if rc:
+            raise _err(rc)
+        return [r.as_dict() for r in per], tot.as_dict()
+
+    def release(self):
+        if self.handle:
+            lib().kplex_release(self.handle)
+            self.handle = None
+
+
+def _jobs(graphs, truss=0):
+    keep = []
+    jobs = (Job * len(graphs))()
+    for i, (off, adj, k, q) in enumerate(graphs):
+        off = np.ascontiguousarray(off, dtype=np.uint32)
+        adj = np.ascontiguousarray(adj if len(adj) else np.zeros(1, np.uint32), dtype=np.uint32)
+        keep.append((off, adj))
+        jobs[i] = Job(_u32p(off), _u32p(adj), len(off) - 1, int(off[-1]), k, q, truss)
+    return jobs, keep
+
+
+def enumerate_batch(graphs, thres: float = 0.25, truss: int = 0, flags: int = FLAG_QUIET, device: int = 0,
+                    pool_slots: int = 0):
+    """graphs: list of (offsets, neighbors, k, q).  Returns (per-graph results, totals)."""
+    jobs, keep = _jobs(graphs, truss)
+    p = make_params(2, 3, thres, 0, flags, device, pool_slots)
+    per = (Result * len(graphs))()
+    tot = Result()
+    rc = lib().kplex_enumerate_batch(jobs, len(graphs), ctypes.byref(p), per, ctypes.byref(tot))
+    if rc:
+        raise _err(rc)
+    return [r.as_dict() for r in per], tot.as_dict()
+
+
+def prepare_batch(graphs, thres: float = 0.25, truss: int = 0, flags: int = FLAG_QUIET, device: int = 0,
+                  pool_slots: int = 0) -> PreparedBatch:
+    jobs, keep = _jobs(graphs, truss)
+    p = make_params(2, 3, thres, 0, flags, device, pool_slots)
+    h = ctypes.c_void_p()
+    tot = Result()
+    rc = lib().kplex_prepare_batch(jobs, len(graphs), ctypes.byref(p), ctypes.byref(h), ctypes.byref(tot))
+    if rc:
+        raise _err(rc)
+    return PreparedBatch(h, len(graphs), tot.as_dict())
 
 
 def device_ok(device: int = 0) -> bool:

@@ -1,0 +1,35 @@
+"""Batched enumeration: many graphs with mixed k and q in one persistent launch.
+
+Per-graph counts and hashes must equal separate single-graph calls (and the
+oracle), bit for bit."""
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def test_batch_matches_single_calls(kp, orc):
+    graphs = kp.batch_workload(count=48, seed=4)
+    per, tot = kp.enumerate_batch(graphs)
+    assert tot["status"] == 0
+    assert sum(r["count"] for r in per) == tot["count"]
+    for i, (off, adj, k, q) in enumerate(graphs):
+        one = kp.enumerate_csr(off, adj, k, q)
+        assert (per[i]["count"], per[i]["hash"], per[i]["valid_roots"]) == (one["count"], one["hash"], one["valid_roots"]), i
+        if i % 8 == 0:
+            o = orc.enumerate_csr(off, adj, k, q)
+            assert (o["count"], o["hash"]) == (one["count"], one["hash"])
+
+
+def test_batch_reuse_and_mixed_sizes(kp, orc):
+    small = kp.workload_graph("small")
+    graphs = [(small[0], small[1], 2, 8)] + kp.batch_workload(count=7, seed=9) + [(small[0], small[1], 3, 9)]
+    prep = kp.prepare_batch(graphs)
+    try:
+        a_per, a_tot = prep.search()
+        b_per, b_tot = prep.search()
+        assert [(r["count"], r["hash"]) for r in a_per] == [(r["count"], r["hash"]) for r in b_per]
+    finally:
+        prep.release()
+    assert a_per[0]["count"] == 871
+    o = orc.enumerate_csr(small[0], small[1], 3, 9)
+    assert (a_per[-1]["count"], a_per[-1]["hash"]) == (o["count"], o["hash"])

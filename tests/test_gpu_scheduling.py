@@ -80,3 +80,19 @@ def test_oversized_root_is_an_error(kp):
     assert g["status"] == kp.ERR_CAPACITY
     small = kp.workload_graph("small")
     assert kp.enumerate_csr(*small, 2, 8)["count"] > 0
+
+
+@pytest.mark.parametrize("slots", [128, 1024])
+def test_spill_to_host_same_result(kp, orc, slots):
+    """With KPLEX_FLAG_SPILL_HOST a small device pool overflows into pinned host
+    memory instead of pausing k-search; idle warps refill from it.  The
+    enumeration is unchanged (the reference's spill/refill, host:168-251, is dead code)."""
+    off, adj = _dense(orc)
+    full = kp.enumerate_csr(off, adj, 3, 8)
+    g = kp.enumerate_csr(off, adj, 3, 8, thres=0.25, pool_slots=slots, flags=kp.FLAG_QUIET | kp.FLAG_SPILL_HOST)
+    assert (g["count"], g["hash"], g["tasks"]) == (full["count"], full["hash"], full["tasks"])
+    assert g["spilled"] > 0
+    w = kp.WORKLOADS["small"]
+    so, sa = kp.workload_graph("small")
+    a = kp.enumerate_csr(so, sa, w["k"], w["q"], pool_slots=64, flags=kp.FLAG_QUIET | kp.FLAG_SPILL_HOST)
+    assert a["count"] == 871
