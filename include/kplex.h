@@ -149,6 +149,22 @@ long long kplex_preprocess_csr(const uint32_t* offsets, const uint32_t* neighbor
                                uint32_t* out_off, uint32_t* out_adj, int32_t* out_dpos, int32_t* out_dseq,
                                uint32_t* out_orig, uint64_t* out_m);
 
+/* No reference counterpart: added for callers that cannot allocate device memory
+ * (device memory fully reserved by another allocator, a fixed memory plan with
+ * no allocation on the request path, or no tolerance for the synchronisation
+ * an allocation can cause).  Runs decomposition + k-search + branch-and-bound
+ * with every scratch buffer carved from one 64 MiB __device__ array inside the
+ * library; calls no cudaMalloc/cudaFree.  Inputs are the pruned graph from
+ * kplex_preprocess_csr in caller-owned device buffers (offsets, neighbors,
+ * dpos, dseq, pruned->input ids, pn vertices); the result goes to *out.
+ * Graphs whose scratch exceeds 64 MiB are rejected with KPLEX_ERR_NOMEM.  The
+ * first call on a device looks up the array's device address (make it before
+ * any stream capture); calls share the array, so calls that overlap on one
+ * GPU race. */
+int kplex_search_noalloc(const uint32_t* d_offsets, const uint32_t* d_neighbors, const int32_t* d_dpos,
+                         const int32_t* d_dseq, const uint32_t* d_orig, uint32_t pn,
+                         const kplex_params* p, kplex_result* out);
+
 /* Batched enumeration (no reference counterpart; the reference handles one
  * graph per process).  Each job is an independent graph with its own k, q and
  * truss setting; thres, flags, device and pool size come from `common`.  All
