@@ -32,6 +32,10 @@ import numpy as np  # noqa: E402
 import kplex_b200 as kp  # noqa: E402
 
 METRIC = "maximal k-plexes/sec"
+# The reference's headline graph (its README's soc-Epinions1 run, k=4, q=30).
+# The epinions-shaped synthetic graph of the same size holds too many plexes
+# to enumerate in a bench step, so it is a named workload only.
+DEFAULT_WORKLOAD = os.path.join(ROOT, "datasets", "soc-epinions.bin") + ":4:30:0"
 UNIT = "plexes/s"
 
 
@@ -45,8 +49,15 @@ def load_workload(name: str):
     # a real .bin graph: name = path:k:q:truss
     path, k, q, tr = name.split(":")
     off, adj = kp.load_bin(path)
-    return off, adj, dict(workload=os.path.basename(path), n=int(len(off) - 1), m_directed=int(len(adj)),
+    return off, adj, dict(workload=os.path.basename(path) + f" k={k} q={q} truss={tr}", n=int(len(off) - 1),
+                          m_directed=int(len(adj)),
                           k=int(k), q=int(q), t=0.25, truss=int(tr))
+
+
+def data_kind(cfg) -> str:
+    if "synthetic" in cfg["workload"]:
+        return "synthetic (seeded Chung-Lu + planted dense groups)"
+    return "real graph file (.bin)"
 
 
 def measured_peak():
@@ -160,7 +171,7 @@ def run_reference(args, cfg, off, adj):
     v = statistics.median([s["value"] for s in steps])
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "u32",
-            "data": "synthetic (seeded Chung-Lu + planted dense groups)" if "synthetic" in cfg["workload"] else "file",
+            "data": data_kind(cfg),
             "config": cfg, "cpu_baseline": {**steps[-1], "value": v},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -172,11 +183,15 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="epinions")
+    ap.add_argument("--workload", default=None,
+                    help="a named synthetic workload (small, epinions, email) or path:k:q:truss; default: "
+                         "the soc-Epinions1 graph at k=4, q=30 when datasets/ holds it, else small")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
+    if args.workload is None:
+        args.workload = DEFAULT_WORKLOAD if os.path.exists(DEFAULT_WORKLOAD.split(":")[0]) else "small"
 
     off, adj, cfg = load_workload(args.workload)
     if args.impl == "reference":
@@ -259,7 +274,7 @@ def main():
     if os.path.exists(prof):
         with open(prof) as f:
             pj = json.load(f)
-        if pj.get("workload") == args.workload:
+        if pj.get("workload") == cfg["workload"]:
             traffic = pj.get("dram_bytes_per_launch")
 
     line = {
@@ -268,7 +283,7 @@ def main():
         "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True, "scaling": "strong",
         "vs_baseline": None, "dtype": "u32",
-        "data": "synthetic (seeded Chung-Lu + planted dense groups)" if "synthetic" in cfg["workload"] else "file",
+        "data": data_kind(cfg),
         "config": cfg,
         "count": total_count, "hash": f"{total_hash:#018x}", "results_consistent": consistent,
         "roofline": {"bound": "hbm", "kernel": "bnb_kernel", "achieved": achieved, "peak": peak,

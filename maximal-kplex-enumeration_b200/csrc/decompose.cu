@@ -32,12 +32,12 @@ struct DecompScratch {
     uint32_t* later;    // MAX_LOCAL
     uint32_t* earlier;  // MAX_LOCAL
     uint32_t* blk;      // MAX_LOCAL + 32 (root, C1, C2)
-    uint32_t* left;     // 2 * MAX_LOCAL + 32
-    uint32_t* tmp;      // 2 * MAX_LOCAL + 32
+    uint32_t* left;     // MAX_LEFT + 32
+    uint32_t* tmp;      // MAX_LEFT + 32
 };
 
 __host__ __device__ inline uint64_t decomp_scratch_words(uint32_t pn) {
-    return 2ull * pn + 2 * MAX_LOCAL + (MAX_LOCAL + 32) + 2 * (2 * MAX_LOCAL + 32) + 64;
+    return 2ull * pn + 2 * MAX_LOCAL + (MAX_LOCAL + 32) + 2 * (MAX_LEFT + 32) + 64;
 }
 
 __device__ inline DecompScratch decomp_scratch(const SearchParams& sp, unsigned warp) {
@@ -48,7 +48,7 @@ __device__ inline DecompScratch decomp_scratch(const SearchParams& sp, unsigned 
     s.later = b; b += MAX_LOCAL;
     s.earlier = b; b += MAX_LOCAL;
     s.blk = b; b += MAX_LOCAL + 32;
-    s.left = b; b += 2 * MAX_LOCAL + 32;
+    s.left = b; b += MAX_LEFT + 32;
     s.tmp = b;
     return s;
 }
@@ -64,7 +64,7 @@ __device__ __forceinline__ int count_local_nbrs(const SearchParams& sp, const ui
     return warp_sum(c);
 }
 
-// Stable rank sort of m distinct values (m <= 2 * MAX_LOCAL) from src into dst.
+// Rank sort of m distinct values (m <= MAX_LEFT) from src into dst.
 __device__ void rank_sort(const uint32_t* src, uint32_t* dst, int m) {
     const unsigned l = lane_id();
     __syncwarp();
@@ -82,7 +82,7 @@ __global__ void __launch_bounds__(256) decompose_kernel(SearchParams sp) {
     const unsigned warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     DecompScratch S = decomp_scratch(sp, warp);
     __shared__ uint32_t s_alive_all[8][MAX_WORDS];
-    __shared__ uint32_t s_row_all[8][2 * MAX_WORDS];
+    __shared__ uint32_t s_row_all[8][MAX_WORDS + MAX_LEFT_WORDS];
     uint32_t* s_alive = s_alive_all[threadIdx.x >> 5];
     uint32_t* s_row = s_row_all[threadIdx.x >> 5];
 
@@ -231,7 +231,7 @@ __global__ void __launch_bounds__(256) decompose_kernel(SearchParams sp) {
             __syncwarp();
             int nc2 = 0, nl2 = 0;
             const int cap2 = MAX_LOCAL - hop + 1;    // one past the limit to detect overflow
-            const int capl = 2 * MAX_LOCAL - nl1;
+            const int capl = MAX_LEFT + 1 - nl1;   // one past the limit to detect overflow
             for (int i = 1; i < hop; ++i) {
                 const uint32_t c1v = S.blk[i];
                 for (uint32_t b = sp.off[c1v]; b < sp.off[c1v + 1]; b += 32) {
@@ -259,7 +259,7 @@ __global__ void __launch_bounds__(256) decompose_kernel(SearchParams sp) {
             __syncwarp();
             n = hop + nc2;
             nleft = nl1 + nl2;
-            if (n > MAX_LOCAL || nleft > MAX_LOCAL) oversized = true;
+            if (n > MAX_LOCAL || nleft > MAX_LEFT) oversized = true;
             if (!oversized) {
                 rank_sort(S.tmp, S.blk + hop, nc2);                 // C2 ascending
                 for (int i = l; i < nleft; i += 32) S.tmp[i] = S.left[i];
@@ -294,8 +294,7 @@ __global__ void __launch_bounds__(256) decompose_kernel(SearchParams sp) {
                 __threadfence_block();
                 // A, LA, LT rows (src:405-443)
                 for (int i = 0; i < n; ++i) {
-                    s_row[l] = 0u;
-                    s_row[MAX_WORDS + l] = 0u;
+                    for (uint32_t w = l; w < MAX_WORDS + WL; w += 32) s_row[w] = 0u;
                     __syncwarp();
                     const uint32_t u = S.blk[i];
                     for (uint32_t j = sp.off[u] + l; j < sp.off[u + 1]; j += 32) {
@@ -309,7 +308,7 @@ __global__ void __launch_bounds__(256) decompose_kernel(SearchParams sp) {
                     }
                     __syncwarp();
                     if (l < W) A[(uint64_t)i * W + l] = s_row[l];
-                    if (l < WL) LA[(uint64_t)i * WL + l] = s_row[MAX_WORDS + l];
+                    for (uint32_t w = l; w < WL; w += 32) LA[(uint64_t)i * WL + w] = s_row[MAX_WORDS + w];
                     __syncwarp();
                 }
                 __threadfence_block();

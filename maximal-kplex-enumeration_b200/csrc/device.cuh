@@ -25,6 +25,12 @@ namespace kplex {
 
 constexpr int MAX_LOCAL = 1024;     // inc/common.h:8 MAX_BLK_SIZE
 constexpr int MAX_WORDS = MAX_LOCAL / 32;
+// The left set (earlier-ordered vertices that may extend an output) is only
+// read by the maximality check, so it may be larger than the local subgraph;
+// the reference's left buffers and its 1024-bit `uni` mask stop at 1024
+// (src:117-121, 262, 706-841).
+constexpr int MAX_LEFT = 8192;
+constexpr int MAX_LEFT_WORDS = MAX_LEFT / 32;
 constexpr int KS_MAX_DEPTH = 1000;  // inc/common.h:15 MAX_DEPTH
 constexpr int MAX_K = 32;
 

@@ -98,8 +98,10 @@ extern "C" int kplex_search_noalloc(const uint32_t* d_off, const uint32_t* d_adj
     const long long lim = (long long)pn - (long long)p->q + 2;   // src:44-45
     const uint32_t nroots = lim > 0 ? (uint32_t)std::min<long long>(lim, pn) : 0u;
     // ---- layout, phase 1: counters | pool header | roots | job prefix | arena ... | decomposition scratch (at the end)
-    const uint32_t dec_warps = std::max<uint32_t>(8, std::min<uint32_t>((uint32_t)sms * 2, ((nroots + 7) / 8) * 8));
     const uint64_t scratch_words = decomp_scratch_words_host(pn);
+    // decomposition warps: two per SM, fewer when their scratch would take over half the array
+    uint32_t dec_warps = std::max<uint32_t>(8, std::min<uint32_t>((uint32_t)sms * 2 / 8 * 8, ((nroots + 7) / 8) * 8));
+    while (dec_warps > 8 && (size_t)dec_warps * scratch_words * 4 > NOALLOC_BYTES / 2) dec_warps = std::max<uint32_t>(8, dec_warps / 16 * 8);
     size_t off = 0;
     Counters* ctr = reinterpret_cast<Counters*>(base + off); off = align_up(off + sizeof(Counters), 256);
     Pool* pool = reinterpret_cast<Pool*>(base + off); off = align_up(off + sizeof(Pool), 256);

@@ -440,42 +440,48 @@ __device__ bool left_maximal(const SearchParams& sp, const RootView& R, const Bn
     const int k = R.k;
     if (R.nleft == 0) return true;
     const uint32_t WL = R.WL, W = R.W;
-    uint32_t lc = 0;
-    if (l < WL) {
-        const int lo = (int)l * 32, nl = (int)R.nleft;
-        lc = nl >= lo + 32 ? FULL : (nl > lo ? ((1u << (nl - lo)) - 1) : 0u);
-    }
-    for (int b = 0; b < s; b += 32) {
-        const int i = b + (int)l;
-        const bool sat = i < s && (int)deg[i] + k <= s;
-        unsigned msk = __ballot_sync(FULL, sat);
-        while (msk) {
-            const int j = __ffs(msk) - 1;
-            msk &= msk - 1;
-            const uint32_t u = m.list[b + j];
-            if (l < WL) lc &= __ldg(R.LA + (uint64_t)u * WL + l);
-        }
-    }
-    uint32_t un = 0;
-    for (int t = 0; t < k && t < s; ++t) {
-        const uint32_t u = m.list[t];
-        if (l < WL) un |= __ldg(R.LA + (uint64_t)u * WL + l);
-    }
-    lc &= un;
-    bool found = false;
-    uint32_t c = lc;
     int nrows = 0;
-    while (c && !found) {
-        const int b = __ffs(c) - 1;
-        c &= c - 1;
-        const uint32_t j = l * 32 + b;
-        const int cnt = row_and_popc(R.LT + (uint64_t)j * W, sS, W);
-        ++nrows;
-        if (cnt + k >= s + 1) found = true;
+    bool found = false;
+    // the left set's words in chunks of 32, one word per lane
+    for (uint32_t base = 0; base < WL && !found; base += 32) {
+        const uint32_t w = base + l;
+        uint32_t lc = 0;
+        if (w < WL) {
+            const int lo = (int)w * 32, nl = (int)R.nleft;
+            lc = nl >= lo + 32 ? FULL : (nl > lo ? ((1u << (nl - lo)) - 1) : 0u);
+        }
+        for (int b = 0; b < s; b += 32) {   // adjacent to every saturated member
+            const int i = b + (int)l;
+            const bool sat = i < s && (int)deg[i] + k <= s;
+            unsigned msk = __ballot_sync(FULL, sat);
+            while (msk) {
+                const int j = __ffs(msk) - 1;
+                msk &= msk - 1;
+                const uint32_t u = m.list[b + j];
+                if (w < WL) lc &= __ldg(R.LA + (uint64_t)u * WL + w);
+            }
+        }
+        uint32_t un = 0;   // and to one of any k members
+        for (int t = 0; t < k && t < s; ++t) {
+            const uint32_t u = m.list[t];
+            if (w < WL) un |= __ldg(R.LA + (uint64_t)u * WL + w);
+        }
+        lc &= un;
+        bool f = false;
+        uint32_t c = lc;
+        while (c && !f) {
+            const int bit = __ffs(c) - 1;
+            c &= c - 1;
+            const uint32_t j = w * 32 + bit;
+            const int cnt = row_and_popc(R.LT + (uint64_t)j * W, sS, W);
+            ++nrows;
+            if (cnt + k >= s + 1) f = true;
+        }
+        found = __any_sync(FULL, f);
     }
     nrows = warp_sum(nrows);
     if (l == 0) bb += (unsigned long long)nrows * 4ull * W + (unsigned long long)(k + 1) * 4ull * WL;
-    return !__any_sync(FULL, found);
+    return !found;
 }
 
 // Adds one maximal k-plex (list[0..s)) to the count and hash.

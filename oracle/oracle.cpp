@@ -75,6 +75,9 @@ enum : uint8_t { LP = 0, LC = 1, LX = 2, LU = 3, LH = 5 };                 // co
 enum : uint8_t { UNLINK2LESS = 0, LINK2LESS = 1, UNLINK2EQUAL = 2, LINK2EQUAL = 3, UNLINK2MORE = 4, LINK2MORE = 5 };  // common.h:37-44
 
 static const int MAX_BLK = 1024;   // common.h:8
+// Left sets may exceed MAX_BLK (the reference's buffers stop there); the
+// device build accepts up to 8192, so the oracle does too.
+static const int MAX_LEFT = 8192;
 static const int MAX_DEPTH = 1000; // common.h:15
 
 struct Params { int k, q, truss; };
@@ -294,7 +297,7 @@ static bool decompose_root(const Graph& g, const std::vector<int>& dpos, const s
     s.n = n; s.nleft = (int)left.size();
     if (n < q) return false;
     st.valid++;
-    if (n > MAX_BLK || (int)left.size() > MAX_BLK) { st.too_big++; return false; }
+    if (n > MAX_BLK || (int)left.size() > MAX_LEFT) { st.too_big++; return false; }
     {
         uint32_t cur = st.max_n.load(); while ((uint32_t)n > cur && !st.max_n.compare_exchange_weak(cur, n)) {}
         cur = st.max_left.load(); while ((uint32_t)left.size() > cur && !st.max_left.compare_exchange_weak(cur, (uint32_t)left.size())) {}
@@ -362,7 +365,7 @@ struct Ctx {
     std::vector<uint16_t> sat, commons;
     std::vector<uint32_t> uni;
     Ctx(const Sub& s_, const Params& p_, const std::vector<uint32_t>& o, Stats& st_) : s(s_), P(p_), orig(o), st(st_) {
-        sat.resize(MAX_BLK); commons.resize(MAX_BLK); uni.assign(32, 0);
+        sat.resize(MAX_BLK); commons.resize(MAX_LEFT); uni.assign(MAX_LEFT / 32, 0);
     }
 };
 
@@ -730,27 +733,45 @@ static Result run(const Graph& g0, const Params& P, int threads, uint64_t root_b
     const std::vector<uint32_t>* OR = &orig; Stats* ST = &st; const Params* PP = &P;
     std::atomic<uint64_t>* TC = &tot_cnt; std::atomic<uint64_t>* TH = &tot_hash; std::atomic<uint64_t>* TT = &tot_tasks;
     const bool seq = sequential_ksearch;
+    // Branch-and-bound tasks are deferred while fewer than `max_out` wait to run
+    // and run inline in the producing k-search otherwise, so memory stays bounded
+    // on roots that produce millions of tasks.
+    std::atomic<int> outstanding{0};
+    std::atomic<int>* OUT = &outstanding;
+    const int max_out = 8 * std::max(1, omp_get_max_threads());
 #pragma omp parallel
 #pragma omp single
     {
         for (uint64_t ri = rb; ri < re; ++ri) {
             if (shard_count > 1 && ri % shard_count != shard_index) continue;
-#pragma omp task firstprivate(ri, PG, DP, DS, OR, ST, PP, TC, TH, TT, seq)
+#pragma omp task firstprivate(ri, PG, DP, DS, OR, ST, PP, TC, TH, TT, OUT, seq, max_out)
             {
                 std::shared_ptr<Sub> sub = std::make_shared<Sub>();
                 if (decompose_root(*PG, *DP, *DS, (uint32_t)ri, *PP, *sub, *ST)) {
-                    uint64_t kt = 0;
-                    std::vector<std::shared_ptr<Task>> produced;
-                    auto keep = [&produced](Task& t) { produced.push_back(std::make_shared<Task>(std::move(t))); };
-                    if (seq) ksearch(*sub, *PP, *ST, kt, keep);
-                    else for (int d = 0; d <= sub->n - sub->hop; ++d) ksearch(*sub, *PP, *ST, kt, keep, d);
-                    *TT += kt;
-                    for (auto& tp : produced) {
-#pragma omp task firstprivate(tp, sub, OR, ST, PP, TC, TH, TT)
+                    const int njobs = seq ? 1 : sub->n - sub->hop + 1;
+                    for (int d = 0; d < njobs; ++d) {
+#pragma omp task firstprivate(d, sub, OR, ST, PP, TC, TH, TT, OUT, seq, max_out)
                         {
-                            Ctx c(*sub, *PP, *OR, *ST);
-                            bnb(c, *tp);
-                            *TC += c.cnt; *TH += c.hsum; *TT += c.tasks;
+                            uint64_t kt = 0;
+                            Ctx inl(*sub, *PP, *OR, *ST);
+                            auto sink = [&](Task& t) {
+                                if (OUT->load(std::memory_order_relaxed) < max_out) {
+                                    OUT->fetch_add(1);
+                                    std::shared_ptr<Task> tp = std::make_shared<Task>(std::move(t));
+#pragma omp task firstprivate(tp, sub, OR, ST, PP, TC, TH, TT, OUT)
+                                    {
+                                        Ctx c(*sub, *PP, *OR, *ST);
+                                        bnb(c, *tp);
+                                        *TC += c.cnt; *TH += c.hsum; *TT += c.tasks;
+                                        OUT->fetch_sub(1);
+                                    }
+                                } else {
+                                    bnb(inl, t);
+                                }
+                            };
+                            if (seq) ksearch(*sub, *PP, *ST, kt, sink);
+                            else ksearch(*sub, *PP, *ST, kt, sink, d);
+                            *TC += inl.cnt; *TH += inl.hsum; *TT += inl.tasks + kt;
                         }
                     }
                 }

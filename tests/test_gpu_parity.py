@@ -50,6 +50,15 @@ def test_random_vs_oracle(kp, orc, k, truss):
             assert (g["count"], g["hash"], g["tasks"]) == (o["count"], o["hash"], o["tasks"]), (seed, k, q)
 
 
+def test_left_sets_beyond_1024(kp, orc):
+    from conftest import big_left_graph
+    off, adj = big_left_graph()
+    g = kp.enumerate_csr(off, adj, 2, 4)
+    o = orc.enumerate_csr(off, adj, 2, 4, threads=4)
+    assert g["max_left"] == o["max_left"] > 1024
+    assert (g["count"], g["hash"], g["tasks"]) == (o["count"], o["hash"], o["tasks"])
+
+
 def test_edge_cases(kp):
     # empty graph, no vertex survives the core, graph too small for any root
     off = np.zeros(1, np.uint32)

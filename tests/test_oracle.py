@@ -87,3 +87,15 @@ def test_golden_datasets_match_readme():
     assert d["soc-epinions.bin:4:30:0"]["count"] == 13172906   # README.md:142
     assert d["email-euall.bin:3:12:0"]["count"] == 32639016    # README.md:144
     assert d["email-euall.bin:3:12:1"]["count"] == 32639016
+
+
+def test_oracle_left_sets_beyond_1024(orc):
+    # the reference's left buffers stop at 1024; the oracle (like the device
+    # build) accepts up to 8192 and both k-search schedules agree there
+    from conftest import big_left_graph
+    off, adj = big_left_graph()
+    a = orc.enumerate_csr(off, adj, 2, 4, threads=4)
+    b = orc.enumerate_sequential(off, adj, 2, 4, threads=4)
+    assert a["max_left"] > 1024 and a["oversized_roots"] == 0
+    assert (a["count"], a["hash"]) == (b["count"], b["hash"])
+    assert a["count"] == 629841
