@@ -177,6 +177,161 @@ def run_reference(args, cfg, off, adj):
     print(json.dumps(line), flush=True)
 
 
+def _pct(xs, p):
+    xs = sorted(xs)
+    if not xs:
+        return 0.0
+    i = min(len(xs) - 1, max(0, int(round(p / 100.0 * (len(xs) - 1)))))
+    return xs[i]
+
+
+def run_batched(args):
+    """4,096 seeded graphs (n log-uniform in [64, 2048], mixed k and q) in one launch,
+    on the autotuned schedule, against one plain launch per graph."""
+    import torch
+    torch.cuda.set_device(0)
+    graphs = kp.batch_workload(args.batch_count, 4, min_q_k4=0 if args.batch_full else 12)
+    tuned, tune_ms = kp.autotune_batch(graphs, sample=min(256, len(graphs)))
+    prep = kp.prepare_batch(graphs, **tuned)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda:0")
+    for _ in range(args.warmup):
+        prep.search()
+        flush.zero_()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(0)
+    sampler.start()
+    res = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        res.append(prep.search())
+    clocks = sampler.stop()
+    prep.release()
+    per, tot = res[-1]
+    dev_ms = sum(t["ms_device"] for _, t in res)
+    # end to end: host preprocessing of every graph, upload, search, per-graph results
+    t0 = time.perf_counter()
+    per_e2e, tot_e2e = kp.enumerate_batch(graphs, **tuned)
+    e2e_ms = (time.perf_counter() - t0) * 1e3
+    # one plain launch per graph, back to back
+    t0 = time.perf_counter()
+    seq = [kp.enumerate_csr(o, a, k, q) for (o, a, k, q) in graphs]
+    seq_ms = (time.perf_counter() - t0) * 1e3
+    exact = all((per[i]["count"], per[i]["hash"]) == (seq[i]["count"], seq[i]["hash"]) ==
+                (per_e2e[i]["count"], per_e2e[i]["hash"]) for i in range(len(graphs)))
+    count = tot["count"]
+    h2d = sum(4 * (len(o) + len(a)) for (o, a, _, _) in graphs)
+    line = {"metric": METRIC + " (batched)", "value": count * args.steps / (dev_ms / 1e3), "unit": UNIT,
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic (seeded Chung-Lu + planted dense groups)",
+            "config": {"workload": f"{len(graphs)} graphs, seed 4, n log-uniform [64, 2048], k in {{2,3,4}}, q in [8, 20]"
+                                   + ("" if args.batch_full else ", q raised to >= 12 on the k=4 graphs"),
+                       "schedule": tuned, "autotune_sample_ms": tune_ms, "l2": "256 MiB flush between steps"},
+            "count": count, "exact_vs_plain": exact,
+            "e2e": {"value": count / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": 20 * len(graphs), "ms_per_step": e2e_ms},
+            "sequential_plain": {"value": count / (seq_ms / 1e3), "unit": UNIT, "ms": seq_ms,
+                                 "launches": len(graphs)},
+            "batched_e2e_over_sequential": seq_ms / e2e_ms,
+            "gpu_launches": sum(t["gpu_launches"] for _, t in res), "clocks": clocks}
+    print(json.dumps(line), flush=True)
+
+
+def served_requests(rate: float, duration: float, seed: int = 5):
+    """Open-loop Poisson arrivals: 95% graphs drawn as in the batched workload, 5% the
+    epinions graph (the shipped soc-Epinions1 when datasets/ holds it, else the small
+    synthetic graph) at q=30 with k in {2, 3, 4}."""
+    rng = np.random.default_rng(seed)
+    times = []
+    t = 0.0
+    while True:
+        t += float(rng.exponential(1.0 / rate))
+        if t >= duration:
+            break
+        times.append(t)
+    small = kp.batch_workload(len(times), seed)
+    epi = DEFAULT_WORKLOAD.split(":")[0]
+    big = kp.load_bin(epi) if os.path.exists(epi) else kp.workload_graph("small")
+    big_name = "soc-epinions.bin" if os.path.exists(epi) else "small synthetic"
+    reqs = []
+    for i, at in enumerate(times):
+        if rng.random() < 0.05:
+            k = int(rng.integers(2, 5))
+            reqs.append((at, big[0], big[1], k, 30 if big_name == "soc-epinions.bin" else 2 * k + 4, "large"))
+        else:
+            o, a, k, q = small[i]
+            reqs.append((at, o, a, k, q, "small"))
+    return reqs, big_name
+
+
+def run_served(args):
+    """Continuous batching server under an open-loop Poisson stream, against one
+    request at a time through plain launches (FIFO queueing from the measured
+    service times on the same arrival schedule)."""
+    import torch
+    torch.cuda.set_device(0)
+    reqs, big_name = served_requests(args.rate, args.duration)
+    # warm the library and both paths
+    kp.enumerate_csr(reqs[0][1], reqs[0][2], reqs[0][3], reqs[0][4])
+    done = {}
+    sampler = ClockSampler(0)
+    with kp.Server(slots=args.slots, max_batch=args.max_batch, split_grid=args.split_grid,
+                   mem_budget=args.mem_budget << 30) as srv:
+        sampler.start()
+        t0 = time.perf_counter()
+        for i, (at, o, a, k, q, _) in enumerate(reqs):
+            now = time.perf_counter() - t0
+            if at > now:
+                time.sleep(at - now)
+            srv.submit(o, a, k, q, tag=i)
+            for c in srv.poll(256, 0):
+                done[c["tag"]] = c
+        while len(done) < len(reqs):
+            for c in srv.poll(256, 1000):
+                done[c["tag"]] = c
+        makespan = time.perf_counter() - t0
+        clocks = sampler.stop()
+        st = srv.stats()
+    lat = [done[i]["ms_latency"] for i in range(len(reqs))]
+    total = sum(done[i]["count"] for i in range(len(reqs)))
+    # plain launches, one request at a time
+    svc = []
+    plain = []
+    for (_, o, a, k, q, _) in reqs:
+        t1 = time.perf_counter()
+        r = kp.enumerate_csr(o, a, k, q)
+        svc.append(time.perf_counter() - t1)
+        plain.append((r["count"], r["hash"]))
+    free_at = 0.0
+    lat_seq = []
+    for (at, *_), d in zip(reqs, svc):
+        start = max(at, free_at)
+        free_at = start + d
+        lat_seq.append((free_at - at) * 1e3)
+    seq_makespan = free_at - reqs[0][0] if reqs else 0.0
+    exact = all((done[i]["count"], done[i]["hash"]) == plain[i] for i in range(len(reqs)))
+    line = {"metric": METRIC + " (served)", "value": total / makespan, "unit": UNIT, "n_gpus": 1,
+            "steps": 1, "warmup": 1, "ms_per_step": makespan * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32", "data": "synthetic stream (seeded) + " + big_name,
+            "config": {"workload": f"Poisson {args.rate}/s for {args.duration}s, seed 5, 95% batched-workload graphs, "
+                                   f"5% {big_name} q=30 k in {{2,3,4}}", "requests": len(reqs),
+                       "slots": args.slots, "max_batch": args.max_batch, "split_grid": args.split_grid,
+                       "mem_budget_gib": args.mem_budget},
+            "latency_ms": {"p50": _pct(lat, 50), "p99": _pct(lat, 99), "max": max(lat) if lat else 0},
+            "latency_ms_small": {"p50": _pct([l for l, r in zip(lat, reqs) if r[5] == "small"], 50),
+                                 "p99": _pct([l for l, r in zip(lat, reqs) if r[5] == "small"], 99)},
+            "exact_vs_plain": exact, "count": total, "server": st,
+            "one_at_a_time": {"value": total / seq_makespan if seq_makespan else 0.0, "unit": UNIT,
+                              "latency_ms": {"p50": _pct(lat_seq, 50), "p99": _pct(lat_seq, 99)},
+                              "busy_s": sum(svc)},
+            "e2e": {"value": total / makespan, "unit": UNIT,
+                    "h2d_bytes_per_step": sum(4 * (len(r[1]) + len(r[2])) for r in reqs),
+                    "d2h_bytes_per_step": 88 * len(reqs)},
+            "clocks": clocks}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -189,7 +344,27 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mode", default="plain", choices=["plain", "batched", "served"],
+                    help="plain: one graph per step (the headline); batched: many graphs per launch; "
+                         "served: an open-loop request stream through the server")
+    ap.add_argument("--batch-count", type=int, default=4096)
+    ap.add_argument("--batch-full", action="store_true",
+                    help="batched: keep q < 12 on the k=4 graphs (about 12 billion plexes, hours of GPU time)")
+    ap.add_argument("--rate", type=float, default=20.0, help="served: requests per second")
+    ap.add_argument("--duration", type=float, default=60.0, help="served: seconds of arrivals")
+    ap.add_argument("--slots", type=int, default=2)
+    ap.add_argument("--max-batch", type=int, default=256)
+    ap.add_argument("--split-grid", action="store_true")
+    ap.add_argument("--mem-budget", type=int, default=32, help="served: GiB")
+    ap.add_argument("--shards", type=int, default=1,
+                    help="plain, one GPU: search only the roots of rank r % shards == 0 (a small case for profiling)")
     args = ap.parse_args()
+    if args.mode == "batched" and args.impl == "ours":
+        run_batched(args)
+        return
+    if args.mode == "served" and args.impl == "ours":
+        run_served(args)
+        return
     if args.workload is None:
         args.workload = DEFAULT_WORKLOAD if os.path.exists(DEFAULT_WORKLOAD.split(":")[0]) else "small"
 
@@ -217,8 +392,11 @@ def main():
 
     cfg.update(parallelism=f"root-shard x{world}" if world > 1 else "single GPU",
                l2="256 MiB flush between steps")
+    shard_index, shard_count = (rank, world) if world > 1 else (0, args.shards if args.shards > 1 else 0)
+    if shard_count and world == 1:
+        cfg["shard"] = f"roots r % {shard_count} == 0 only"
     prep = kp.prepare(off, adj, cfg["k"], cfg["q"], cfg["t"], cfg["truss"], device=local,
-                      shard_index=rank if world > 1 else 0, shard_count=world if world > 1 else 0)
+                      shard_index=shard_index, shard_count=shard_count)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
     for _ in range(args.warmup):
         prep.search()
@@ -252,7 +430,7 @@ def main():
     e2e_count = 0
     for _ in range(args.e2e_steps):
         r = kp.enumerate_csr(off, adj, cfg["k"], cfg["q"], cfg["t"], cfg["truss"], device=local,
-                             shard_index=rank if world > 1 else 0, shard_count=world if world > 1 else 0)
+                             shard_index=shard_index, shard_count=shard_count)
         e2e_ms.append(r["ms_total"])
         e2e_count = r["count"]
     if world > 1:
@@ -263,7 +441,7 @@ def main():
         dist.all_reduce(c)
         e2e_total = int(c.item())
     else:
-        e2e_max, e2e_total = statistics.median(e2e_ms), e2e_count
+        e2e_max, e2e_total = (statistics.median(e2e_ms), e2e_count) if e2e_ms else (0.0, 0)
     pr = prep.pre
     h2d = 4 * ((pr["pn"] + 1) + pr["pm"] + 3 * pr["pn"])
 
@@ -293,6 +471,12 @@ def main():
         "e2e": {"value": e2e_total / (e2e_max / 1e3) if e2e_max > 0 else 0.0, "unit": UNIT,
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 512, "ms_per_step": e2e_max},
         "gpu_launches": launches,
+        "device_counters": {x: res[-1][x] for x in ("tasks", "ks_tasks", "nodes", "valid_roots", "max_local_n",
+                                                    "max_left", "pauses", "stage_copies", "roots_bytes", "search_warps")},
+        # share of warp time in branch-and-bound nodes, in k-search, and idle (per warp-second of the launch)
+        "warp_time_share": {x: (res[-1][x + "_warp_ms"] / (res[-1]["search_warps"] * res[-1]["ms_bnb"])
+                                if res[-1]["search_warps"] and res[-1]["ms_bnb"] > 0 else None)
+                            for x in ("bnb", "ks", "idle")},
         "phases_ms_per_step": {"decompose": sum(r["ms_decompose"] for r in res) / args.steps,
                                "ksearch": sum(r["ms_ksearch"] for r in res) / args.steps,
                                "bnb": bnb_ms / args.steps},

@@ -28,8 +28,8 @@ extern "C" {
 #define KPLEX_ERR_FORMAT     3  /* .bin inconsistent with its header, unsorted lists, ids >= n */
 #define KPLEX_ERR_CUDA       4  /* a CUDA runtime call failed */
 #define KPLEX_ERR_NOMEM      5  /* device or host allocation failed / budget too small */
-#define KPLEX_ERR_CAPACITY   6  /* a root's 2-hop subgraph or left set exceeds 1024 vertices
-                                   (the reference's MAX_BLK_SIZE, inc/common.h:8) */
+#define KPLEX_ERR_CAPACITY   6  /* a root's 2-hop subgraph exceeds 1024 vertices (the reference's
+                                   MAX_BLK_SIZE, inc/common.h:8) or its left set 8192 */
 #define KPLEX_ERR_TIMEOUT    7  /* a bounded device-side wait gave up */
 #define KPLEX_ERR_NO_DEVICE  8  /* no CUDA device / extension not usable */
 #define KPLEX_ERR_INTERNAL   9  /* device-side consistency check failed */
@@ -39,8 +39,8 @@ extern "C" {
 #define KPLEX_FLAG_NO_HASH      0x2u  /* skip the per-output hash (count only) */
 #define KPLEX_FLAG_SPILL_HOST   0x4u  /* when the device task pool reaches thres * pool_slots, k-search writes
                                          further tasks to pinned host memory (up to 4x the pool) instead of
-                                         pausing, and idle warps refill from there (north_star spill/refill;
-                                         the reference's spillToHost/reFillTasks are dead code, host:168-251) */
+                                         pausing, and idle warps refill from there (the reference declares
+                                         spillToHost/reFillTasks, host:168-251, but never calls them) */
 #define KPLEX_FLAG_TEST_NO_WAIT 0x8u  /* test hook: branch warps give up every bounded wait at once, so the
                                          run must end with KPLEX_ERR_TIMEOUT instead of hanging */
 
@@ -56,6 +56,9 @@ typedef struct {
     uint32_t omp_threads;   /* host threads for preprocessing (0 = all) */
     uint32_t shard_index;   /* multi-GPU root sharding: this call searches the roots whose */
     uint32_t shard_count;   /* degeneracy rank r has r % shard_count == shard_index (0/0 = all) */
+    uint32_t blocks_per_sm; /* persistent search kernel: 8-warp blocks per SM, 2 or 3 (0 = 2) */
+    int32_t stage_after;    /* branch nodes a warp processes on one root before it copies the root's
+                               adjacency matrix to shared memory (0 = 8, < 0 = never) */
 } kplex_params;
 
 /* Results.  count/hash are the parity outputs; the rest mirrors the
@@ -86,6 +89,9 @@ typedef struct {
     uint64_t ks_tasks;      /* tasks emitted by k-search (the rest of `tasks` are branch children) */
     uint64_t stage_copies;  /* root adjacency matrices copied into shared memory */
     double ks_warp_ms;      /* k-search time summed over producer warps (diagnostic) */
+    double bnb_warp_ms;     /* branch-and-bound time summed over warps (diagnostic) */
+    double idle_warp_ms;    /* time warps spent finding no work, summed (diagnostic) */
+    uint32_t search_warps;  /* warps of the persistent search kernel */
 } kplex_result;
 
 /* A CSR graph owned by the library (kplex_load_bin / kplex_generate). */
@@ -185,6 +191,71 @@ int kplex_enumerate_batch(const kplex_job* jobs, uint32_t njobs, const kplex_par
 int kplex_prepare_batch(const kplex_job* jobs, uint32_t njobs, const kplex_params* common,
                         kplex_prepared** h, kplex_result* total);
 int kplex_search_batch(kplex_prepared* h, kplex_result* per_job, kplex_result* total);
+
+/* Request server (no reference counterpart; the reference runs one graph per
+ * process).  Requests (one graph with its own k, q, truss) are submitted as
+ * they arrive and complete asynchronously.  `slots` worker threads each own a
+ * CUDA stream and a device workspace (arena, task pool, branch stacks, spill
+ * ring); a free slot admits every waiting request that fits the device-memory
+ * budget (up to max_batch) and enumerates them as one batched launch, so
+ * requests arriving while others run join the next launch and launches of
+ * different slots overlap on the device.  A request's result is the same as
+ * kplex_enumerate_csr's on its graph. */
+typedef struct kplex_server kplex_server;
+typedef struct {
+    int device;
+    uint32_t slots;          /* concurrent launches (streams), 0 -> 2 */
+    uint32_t max_batch;      /* requests per launch, 0 -> 1024 */
+    uint64_t mem_budget;     /* device bytes for workspaces + admitted requests (spill ring
+                                included), 0 -> 16 GiB */
+    uint32_t split_grid;     /* 1: each launch gets 1/slots of the SMs; 0: the whole device */
+    float thres;             /* pause threshold, as kplex_params.thres (0 -> 0.25) */
+    uint32_t flags;          /* KPLEX_FLAG_* applied to every launch */
+    uint64_t pool_slots;     /* as kplex_params.pool_slots */
+} kplex_server_config;
+
+typedef struct {
+    uint64_t tag;            /* the submitter's request id */
+    int status;
+    uint32_t batch_size;     /* requests in the launch that served it */
+    uint64_t count, hash;
+    uint64_t valid_roots;
+    uint32_t pn, slot;
+    double ms_queue;         /* submit -> launch start (admission wait) */
+    double ms_service;       /* launch start -> results on the host (preprocess, upload, search) */
+    double ms_latency;       /* submit -> completion */
+} kplex_completion;
+
+typedef struct {
+    uint64_t submitted, completed, rejected, launches;
+    uint64_t device_bytes;        /* workspaces + in-flight requests now */
+    uint64_t peak_device_bytes;
+    uint32_t max_concurrent;      /* most launches in flight at once */
+    uint32_t max_batch_seen;
+} kplex_server_stats;
+
+int kplex_server_create(const kplex_server_config* cfg, kplex_server** out);
+/* Copies the job's CSR; returns KPLEX_OK, or KPLEX_ERR_PARAM / KPLEX_ERR_NOMEM (the
+ * request alone exceeds the budget) without queueing it. */
+int kplex_server_submit(kplex_server* s, const kplex_job* job, uint64_t tag);
+/* Moves up to `max` completions into out; waits up to timeout_ms (-1: until one
+ * arrives or nothing is pending) for the first.  Returns the number moved. */
+int kplex_server_poll(kplex_server* s, kplex_completion* out, uint32_t max, int timeout_ms);
+/* Waits until every submitted request has completed; KPLEX_ERR_TIMEOUT after timeout_ms (-1: no limit). */
+int kplex_server_drain(kplex_server* s, int timeout_ms);
+int kplex_server_stats_get(kplex_server* s, kplex_server_stats* out);
+/* Finishes queued requests, joins the workers and frees the workspaces. */
+void kplex_server_destroy(kplex_server* s);
+
+/* Autotuner for batched runs (no reference counterpart): enumerates a
+ * deterministic sample of `sample` jobs (every njobs/sample-th) under each
+ * candidate schedule (blocks per SM, shared-memory staging point, task-pool
+ * capacity, pause threshold), keeps the fastest by device time, and writes it
+ * to *best (= *common with the tuned fields replaced).  The sample's counts
+ * must agree across candidates, or KPLEX_ERR_INTERNAL is returned.
+ * *best_ms receives the winner's device time on the sample. */
+int kplex_autotune_batch(const kplex_job* jobs, uint32_t njobs, const kplex_params* common, uint32_t sample,
+                         kplex_params* best, double* best_ms);
 
 const char* kplex_status_string(int status);
 /* Text of the last failure on the calling thread (CUDA message, parse error, ...). */

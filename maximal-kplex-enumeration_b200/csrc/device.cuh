@@ -93,6 +93,8 @@ struct Counters {
     unsigned long long ks_cycles;  // SM cycles producers spent in k-search
     unsigned long long spilled;    // records written to the host spill ring
     unsigned long long refilled;   // records read back from it
+    unsigned long long bnb_cycles;   // SM cycles warps spent in branch-and-bound nodes
+    unsigned long long idle_cycles;  // SM cycles warps spent finding no work
 };
 
 // Vyukov bounded MPMC ring: each slot carries a sequence number so that a

@@ -22,7 +22,7 @@
 #include <string>
 #include <vector>
 
-#include "device.cuh"
+#include "engine.h"
 #include "graph_io.h"
 #include "preprocess.h"
 
@@ -56,60 +56,23 @@ __global__ void init_ks_slots(uint32_t* slots, uint32_t nwarps, uint32_t words) 
 // ------------------------------------------------------------------ errors
 static thread_local std::string g_last_error;
 
-#define CK(call)                                                                    \
-    do {                                                                            \
-        cudaError_t e_ = (call);                                                    \
-        if (e_ != cudaSuccess) {                                                    \
-            g_last_error = std::string(#call) + ": " + cudaGetErrorString(e_);      \
-            return KPLEX_ERR_CUDA;                                                  \
-        }                                                                           \
-    } while (0)
+__global__ void search_kernel_2(SearchParams sp, uint32_t nmax);
+__global__ void search_kernel_3(SearchParams sp, uint32_t nmax);
 
-// ------------------------------------------------------------------ device buffer cache
-struct DevBuf {
-    void* p = nullptr;
-    size_t bytes = 0;
-    int ensure(size_t want) {
-        if (want <= bytes && p) return KPLEX_OK;
-        if (p) { cudaFree(p); p = nullptr; bytes = 0; }
-        if (want == 0) want = 16;
-        cudaError_t e = cudaMalloc(&p, want);
-        if (e != cudaSuccess) { cudaGetLastError(); p = nullptr; g_last_error = std::string("cudaMalloc ") + std::to_string(want) + ": " + cudaGetErrorString(e); return KPLEX_ERR_NOMEM; }
-        bytes = want;
-        return KPLEX_OK;
-    }
-    template <typename T> T* as() const { return static_cast<T*>(p); }
-};
-
-// Mapped pinned host memory (cudaHostAllocMapped), grown on demand.
-struct HostMappedBuf {
-    void* h = nullptr;
-    void* d = nullptr;
-    size_t bytes = 0;
-    int ensure(size_t want) {
-        if (want <= bytes && h) return KPLEX_OK;
-        if (h) { cudaFreeHost(h); h = d = nullptr; bytes = 0; }
-        cudaError_t e = cudaHostAlloc(&h, want, cudaHostAllocMapped | cudaHostAllocPortable);
-        if (e == cudaSuccess) e = cudaHostGetDevicePointer(&d, h, 0);
-        if (e != cudaSuccess) { cudaGetLastError(); h = d = nullptr; g_last_error = std::string("pinned host spill buffer: ") + cudaGetErrorString(e); return KPLEX_ERR_NOMEM; }
-        bytes = want;
-        return KPLEX_OK;
-    }
-};
-
-struct DeviceState {
-    bool init = false;
-    int sms = 0;
-    cudaStream_t stream = nullptr;
-    DevBuf roots, ctr, scratch, arena, pool_seq, pool_data, pool, ks, stacks, jobs, spill_ctl, spill_seq;
-    HostMappedBuf spill_data;
-    Counters* h_ctr = nullptr;   // pinned
-};
+int workspace_init(Workspace& w, int device, int sms) {
+    w.device = device;
+    w.sms = sms;
+    CK(cudaStreamCreateWithFlags(&w.stream, cudaStreamNonBlocking));
+    CK(cudaMallocHost(&w.h_ctr, sizeof(Counters)));
+    CK(cudaMallocHost(&w.h_pool, sizeof(Pool)));
+    for (DevBuf* x : w.bufs) x->stream = w.stream;
+    return KPLEX_OK;
+}
 
 static std::mutex g_mu;
 static DeviceState g_dev[64];
 
-static int device_state(int device, DeviceState** out) {
+int device_state(int device, DeviceState** out) {
     if (device < 0 || device >= 64) return KPLEX_ERR_PARAM;
     int n = 0;
     if (cudaGetDeviceCount(&n) != cudaSuccess || device >= n) { cudaGetLastError(); g_last_error = "no CUDA device"; return KPLEX_ERR_NO_DEVICE; }
@@ -120,8 +83,12 @@ static int device_state(int device, DeviceState** out) {
         CK(cudaGetDeviceProperties(&prop, device));
         if (prop.major != 10) { g_last_error = "kernels are built for sm_100a only"; return KPLEX_ERR_NO_DEVICE; }
         d.sms = prop.multiProcessorCount;
-        CK(cudaStreamCreateWithFlags(&d.stream, cudaStreamNonBlocking));
-        CK(cudaMallocHost(&d.h_ctr, sizeof(Counters)));
+        // the dynamic shared-memory cap is raised once to the per-block maximum, so
+        // that concurrent searches never race on a per-function attribute
+        CK(cudaFuncSetAttribute(search_kernel_2, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+        CK(cudaFuncSetAttribute(search_kernel_3, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+        int rc = workspace_init(d.ws, device, d.sms);
+        if (rc) return rc;
         d.init = true;
     }
     *out = &d;
@@ -130,7 +97,7 @@ static int device_state(int device, DeviceState** out) {
 
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 
-static double ms_since(std::chrono::steady_clock::time_point t0) {
+double ms_since(std::chrono::steady_clock::time_point t0) {
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
 
@@ -138,30 +105,40 @@ static double ms_since(std::chrono::steady_clock::time_point t0) {
 
 using namespace kplex;
 
-// A set of preprocessed graphs resident on one device (one graph for
-// kplex_prepare, many for kplex_prepare_batch).  Graph g's pruned vertices are
-// [vbase, vbase + pn) of the concatenated CSR and its roots [root_base,
-// root_base + nroots) of the concatenated root order.
-struct kplex_prepared {
-    int device = 0;
+namespace kplex {
+
+// A prepared set's search captured as one CUDA graph (memsets, decomposition,
+// job prefix, pool init, the persistent search kernel and the result copies),
+// built on the second search of the set once the first has fixed every size
+// (arena, pool, stacks, shared memory, grid) and replayed with one launch and
+// one synchronisation from then on.  Valid while the workspace keeps its
+// buffers (generation) and the set keeps its parameters.
+struct Replay {
+    Workspace* ws = nullptr;
+    uint64_t gen = 0;
     kplex_params p{};
-    uint32_t ngraphs = 0;
-    uint32_t pn = 0, pm = 0, pn_max = 0, nroots = 0;
-    double ms_pre = 0;
-    std::vector<GraphInfo> ginfo;
-    std::vector<uint32_t> gpm;
-    uint32_t* d_off = nullptr;
-    uint32_t* d_adj = nullptr;
-    int32_t* d_dpos = nullptr;
-    int32_t* d_dseq = nullptr;
-    uint32_t* d_orig = nullptr;
-    GraphInfo* d_graphs = nullptr;
-    unsigned long long* d_gcount = nullptr;
-    unsigned long long* d_ghash = nullptr;
-    unsigned int* d_gvalid = nullptr;
+    uint32_t grid_div = 1;
+    SearchParams sp{};
+    uint32_t dec_warps = 0, blocks = 0, nmax = 0, launches = 0;
+    size_t smem = 0;
+    bool minb3 = false;
+    unsigned long long cap = 0, scap = 0;
+    cudaGraphExec_t exec = nullptr;
+    bool exec_per_graph = false;
+    cudaEvent_t ev[6] = {};
+    unsigned long long* h_gc = nullptr;   // pinned per-graph results
+    unsigned long long* h_gh = nullptr;
+    unsigned int* h_gv = nullptr;
+    ~Replay() {
+        if (exec) cudaGraphExecDestroy(exec);
+        for (cudaEvent_t e : ev) if (e) cudaEventDestroy(e);
+        if (h_gc) cudaFreeHost(h_gc);
+        if (h_gh) cudaFreeHost(h_gh);
+        if (h_gv) cudaFreeHost(h_gv);
+    }
 };
 
-static int check_kq(int k, int q) {
+int check_kq(int k, int q) {
     if (k < 2 || k > MAX_K - 1) { g_last_error = "k must be in [2, 31]"; return KPLEX_ERR_PARAM; }
     if (q < 2 * k - 1) { g_last_error = "q must be >= 2k-1"; return KPLEX_ERR_PARAM; }
     return KPLEX_OK;
@@ -175,25 +152,19 @@ static int check_params(const kplex_params* p) {
     return KPLEX_OK;
 }
 
-static void free_prepared(kplex_prepared* h) {
+void free_prepared(kplex_prepared* h) {
     if (!h) return;
     cudaSetDevice(h->device);
-    cudaFree(h->d_off); cudaFree(h->d_adj); cudaFree(h->d_dpos); cudaFree(h->d_dseq); cudaFree(h->d_orig);
-    cudaFree(h->d_graphs); cudaFree(h->d_gcount); cudaFree(h->d_ghash); cudaFree(h->d_gvalid);
+    delete h->replay;
+    void* ps[9] = {h->d_off, h->d_adj, h->d_dpos, h->d_dseq, h->d_orig, h->d_graphs, h->d_gcount, h->d_ghash, h->d_gvalid};
+    for (void* x : ps) if (x) cudaFreeAsync(x, h->stream);
     delete h;
 }
 
-struct HostJob {
-    const uint32_t* off;
-    const uint32_t* adj;
-    uint32_t n;
-    uint64_t m;
-    int k, q, truss;
-};
-
 // Validates, preprocesses (one host thread per graph when there are several)
 // and uploads a set of graphs.
-static int prepare_set(const std::vector<HostJob>& jobs, const kplex_params* p, kplex_prepared** out_h, kplex_result* out) {
+int prepare_set(const std::vector<HostJob>& jobs, const kplex_params* p, Workspace* d, kplex_prepared** out_h,
+                       kplex_result* out) {
     if (!p || !(p->thres > 0.0f) || p->thres > 1.0f) { g_last_error = "thres must be in (0, 1]"; return KPLEX_ERR_PARAM; }
     const size_t G = jobs.size();
     for (const HostJob& j : jobs) {
@@ -201,9 +172,7 @@ static int prepare_set(const std::vector<HostJob>& jobs, const kplex_params* p, 
         if (rc) return rc;
         if (!j.off || (!j.adj && j.m) || (j.n && j.off[j.n] != j.m) || j.m > 0xffffffffull) { g_last_error = "inconsistent CSR"; return KPLEX_ERR_FORMAT; }
     }
-    DeviceState* d = nullptr;
-    int rc = device_state(p->device, &d);
-    if (rc) return rc;
+    CK(cudaSetDevice(d->device));
     auto t0 = std::chrono::steady_clock::now();
     std::vector<Prepped> pres(G);
     std::vector<int> status(G, KPLEX_OK);
@@ -227,7 +196,8 @@ static int prepare_set(const std::vector<HostJob>& jobs, const kplex_params* p, 
     if (G == 1 && !(p->flags & KPLEX_FLAG_QUIET)) printf("\npn = %u\n", pres[0].g.n);
 
     kplex_prepared* h = new kplex_prepared();
-    h->device = p->device;
+    h->device = d->device;
+    h->stream = d->stream;
     h->p = *p;
     h->ngraphs = (uint32_t)G;
     h->ms_pre = ms_pre;
@@ -263,11 +233,10 @@ static int prepare_set(const std::vector<HostJob>& jobs, const kplex_params* p, 
     }
     off[PN] = (uint32_t)PM;
     auto fail = [&](int code) { free_prepared(h); return code; };
-    if (cudaMalloc(&h->d_off, (PN + 1) * 4) != cudaSuccess || cudaMalloc(&h->d_adj, adj.size() * 4) != cudaSuccess ||
-        cudaMalloc(&h->d_dpos, dpos.size() * 4) != cudaSuccess || cudaMalloc(&h->d_dseq, dseq.size() * 4) != cudaSuccess ||
-        cudaMalloc(&h->d_orig, orig.size() * 4) != cudaSuccess || cudaMalloc(&h->d_graphs, G * sizeof(GraphInfo)) != cudaSuccess ||
-        cudaMalloc(&h->d_gcount, G * 8) != cudaSuccess || cudaMalloc(&h->d_ghash, G * 8) != cudaSuccess ||
-        cudaMalloc(&h->d_gvalid, G * 4) != cudaSuccess) {
+    auto dm = [&](auto** ptr, size_t bytes) { return cudaMallocAsync((void**)ptr, bytes, d->stream) == cudaSuccess; };
+    if (!dm(&h->d_off, (PN + 1) * 4) || !dm(&h->d_adj, adj.size() * 4) || !dm(&h->d_dpos, dpos.size() * 4) ||
+        !dm(&h->d_dseq, dseq.size() * 4) || !dm(&h->d_orig, orig.size() * 4) || !dm(&h->d_graphs, G * sizeof(GraphInfo)) ||
+        !dm(&h->d_gcount, G * 8) || !dm(&h->d_ghash, G * 8) || !dm(&h->d_gvalid, G * 4)) {
         cudaGetLastError(); g_last_error = "cudaMalloc for the pruned graphs failed"; return fail(KPLEX_ERR_NOMEM);
     }
     CK(cudaMemcpyAsync(h->d_off, off.data(), off.size() * 4, cudaMemcpyHostToDevice, d->stream));
@@ -286,13 +255,144 @@ static int prepare_impl(const uint32_t* off, const uint32_t* adj, uint32_t n, ui
                         kplex_prepared** out_h, kplex_result* out) {
     int rc = check_params(p);
     if (rc) return rc;
-    return prepare_set({HostJob{off, adj, n, m, p->k, p->q, p->truss}}, p, out_h, out);
+    DeviceState* dev = nullptr;
+    if ((rc = device_state(p->device, &dev))) return rc;
+    return prepare_set({HostJob{off, adj, n, m, p->k, p->q, p->truss}}, p, &dev->ws, out_h, out);
 }
 
-static int search_impl(kplex_prepared* h, kplex_result* out, kplex_result* per_graph = nullptr) {
-    DeviceState* d = nullptr;
-    int rc = device_state(h->device, &d);
-    if (rc) return rc;
+static bool same_params(const kplex_params& a, const kplex_params& b) {
+    return a.k == b.k && a.q == b.q && a.thres == b.thres && a.truss == b.truss && a.flags == b.flags &&
+           a.device == b.device && a.pool_slots == b.pool_slots && a.shard_index == b.shard_index &&
+           a.shard_count == b.shard_count && a.blocks_per_sm == b.blocks_per_sm && a.stage_after == b.stage_after;
+}
+
+static void fill_result(const kplex_prepared* h, const Counters& hc, float ms, double ms_dec, double ms_bnb,
+                        uint32_t launches, uint32_t search_warps, kplex_result* out) {
+    if (!out) return;
+    out->count = hc.count;
+    out->hash = hc.hash;
+    out->valid_roots = hc.valid_roots;
+    out->tasks = hc.tasks;
+    out->nodes = hc.nodes;
+    out->pn = h->pn;
+    out->pm = h->pm;
+    out->max_local_n = hc.max_n;
+    out->max_left = hc.max_left;
+    out->pauses = hc.ks_paused;
+    out->spilled = (uint32_t)std::min<unsigned long long>(hc.spilled, 0xffffffffull);
+    out->ms_preprocess = h->ms_pre;
+    out->ms_device = ms;
+    out->ms_ref_region = h->ms_pre + ms;
+    out->gpu_launches = launches;
+    out->ms_decompose = ms_dec;
+    out->ms_ksearch = 0;
+    out->ms_bnb = ms_bnb;
+    out->bnb_bytes = hc.bnb_bytes;
+    out->roots_bytes = hc.roots_bytes;
+    out->ks_tasks = hc.ks_tasks;
+    out->stage_copies = hc.stage_copies;
+    out->ks_warp_ms = (double)hc.ks_cycles / (1.965e6);   // SM cycles at the 1965 MHz boost clock
+    out->bnb_warp_ms = (double)hc.bnb_cycles / (1.965e6);
+    out->idle_warp_ms = (double)hc.idle_cycles / (1.965e6);
+    out->search_warps = search_warps;
+    out->status = (int)hc.error;
+}
+
+static int replay_capture(kplex_prepared* h, Replay& r, Workspace* d, bool per_graph) {
+    cudaStream_t st = d->stream;
+    const SearchParams& sp = r.sp;
+    const size_t G = h->ngraphs;
+    if (r.exec) { cudaGraphExecDestroy(r.exec); r.exec = nullptr; }
+    for (cudaEvent_t& e : r.ev) if (!e) CK(cudaEventCreate(&e));
+    if (per_graph && !r.h_gc) {
+        CK(cudaMallocHost(&r.h_gc, G * 8));
+        CK(cudaMallocHost(&r.h_gh, G * 8));
+        CK(cudaMallocHost(&r.h_gv, G * 4));
+    }
+    auto kfn = r.minb3 ? search_kernel_3 : search_kernel_2;
+    // events become event-record nodes of the graph (external records), so that the
+    // host can wait on the last one and time the phases after a replay
+    CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    cudaEventRecordWithFlags(r.ev[0], st, cudaEventRecordExternal);
+    cudaMemsetAsync(sp.ctr, 0, sizeof(Counters), st);
+    cudaMemsetAsync(sp.gcount, 0, G * 8, st);
+    cudaMemsetAsync(sp.ghash, 0, G * 8, st);
+    cudaMemsetAsync(sp.gvalid, 0, G * 4, st);
+    if (h->nroots) {
+        init_decomp_scratch<<<d->sms * 4, 256, 0, st>>>(sp.warp_scratch, sp.scratch_words, h->pn_max, r.dec_warps);
+        cudaEventRecordWithFlags(r.ev[1], st, cudaEventRecordExternal);
+        decompose_kernel<<<r.dec_warps / 8, 256, 0, st>>>(sp);
+        cudaEventRecordWithFlags(r.ev[2], st, cudaEventRecordExternal);
+    }
+    job_prefix_kernel<<<1, 1024, 0, st>>>(sp.roots, h->nroots, d->jobs.as<uint32_t>());
+    init_pool<<<d->sms * 4, 256, 0, st>>>(sp.pool_seq, r.cap, sp.pool);
+    if (sp.spill_on) init_pool<<<d->sms * 4, 256, 0, st>>>(sp.spill_seq, r.scap, sp.spill_pool);
+    cudaEventRecordWithFlags(r.ev[3], st, cudaEventRecordExternal);
+    if (h->nroots) kfn<<<r.blocks, 256, r.smem, st>>>(sp, r.nmax);
+    cudaEventRecordWithFlags(r.ev[4], st, cudaEventRecordExternal);
+    cudaMemcpyAsync(d->h_ctr, sp.ctr, sizeof(Counters), cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(d->h_pool, sp.pool, sizeof(Pool), cudaMemcpyDeviceToHost, st);
+    if (per_graph) {
+        cudaMemcpyAsync(r.h_gc, sp.gcount, G * 8, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(r.h_gh, sp.ghash, G * 8, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(r.h_gv, sp.gvalid, G * 4, cudaMemcpyDeviceToHost, st);
+    }
+    cudaEventRecordWithFlags(r.ev[5], st, cudaEventRecordExternal);
+    cudaGraph_t g = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(st, &g);
+    if (ce != cudaSuccess || !g) {
+        cudaGetLastError();
+        g_last_error = std::string("stream capture of the search: ") + cudaGetErrorString(ce);
+        return KPLEX_ERR_CUDA;
+    }
+    const cudaError_t ie = cudaGraphInstantiate(&r.exec, g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) { cudaGetLastError(); r.exec = nullptr; g_last_error = std::string("graph instantiate: ") + cudaGetErrorString(ie); return KPLEX_ERR_CUDA; }
+    r.exec_per_graph = per_graph;
+    return KPLEX_OK;
+}
+
+static int replay_search(kplex_prepared* h, Replay& r, Workspace* d, kplex_result* out, kplex_result* per_graph) {
+    int rc = KPLEX_OK;
+    if (!r.exec || (per_graph && !r.exec_per_graph))
+        if ((rc = replay_capture(h, r, d, per_graph != nullptr))) return rc;
+    CK(cudaGraphLaunch(r.exec, d->stream));
+    CK(cudaEventSynchronize(r.ev[5]));
+    Counters& hc = *d->h_ctr;
+    const Pool& hp = *d->h_pool;
+    float ms = 0, t_dec = 0, t_bnb = 0;
+    CK(cudaEventElapsedTime(&ms, r.ev[0], r.ev[5]));
+    if (h->nroots) CK(cudaEventElapsedTime(&t_dec, r.ev[1], r.ev[2]));
+    CK(cudaEventElapsedTime(&t_bnb, r.ev[3], r.ev[4]));
+    if (!hc.error && hp.head != hp.tail) { hc.error = KPLEX_ERR_TIMEOUT; g_last_error = "branch warps gave up with records left in the pool"; }
+    if (hc.error && g_last_error.empty()) g_last_error = "device error in a replayed search";
+    if (per_graph) {
+        for (size_t g = 0; g < h->ngraphs; ++g) {
+            kplex_result& x = per_graph[g];
+            memset(&x, 0, sizeof x);
+            x.count = r.h_gc[g]; x.hash = r.h_gh[g]; x.valid_roots = r.h_gv[g];
+            x.pn = h->ginfo[g].pn; x.pm = h->gpm[g];
+            x.status = (int)hc.error;
+        }
+    }
+    fill_result(h, hc, ms, t_dec, t_bnb, r.launches, r.blocks * 8, out);
+    return (int)hc.error;
+}
+
+int search_impl(kplex_prepared* h, Workspace* d, kplex_result* out, kplex_result* per_graph, uint32_t grid_div) {
+    int rc = KPLEX_OK;
+    if (h->replay) {
+        Replay& r = *h->replay;
+        if (r.ws == d && r.gen == d->generation() && r.grid_div == grid_div && same_params(r.p, h->p)) {
+            CK(cudaSetDevice(d->device));
+            rc = replay_search(h, r, d, out, per_graph);
+            if (rc) { delete h->replay; h->replay = nullptr; }
+            return rc;
+        }
+        delete h->replay;
+        h->replay = nullptr;
+    }
+    CK(cudaSetDevice(d->device));
     const kplex_params& P = h->p;
     cudaStream_t st = d->stream;
     const uint32_t nroots = h->nroots;
@@ -303,7 +403,7 @@ static int search_impl(kplex_prepared* h, kplex_result* out, kplex_result* per_g
     CK(cudaEventCreate(&ka));
     CK(cudaEventCreate(&kb));
     CK(cudaEventRecord(e0, st));
-    double ms_dec = 0, ms_ks = 0, ms_bnb = 0;
+    double ms_dec = 0, ms_bnb = 0;
     auto timed = [&](auto&& launch, double& acc) -> int {
         CK(cudaEventRecord(ka, st));
         launch();
@@ -360,7 +460,8 @@ static int search_impl(kplex_prepared* h, kplex_result* out, kplex_result* per_g
         break;
     }
     if (hc.error) {
-        g_last_error = hc.error == KPLEX_ERR_CAPACITY ? "a root's 2-hop subgraph or left set exceeds 1024 vertices" : "device error in decomposition";
+        g_last_error = hc.error == KPLEX_ERR_CAPACITY ? "a root's 2-hop subgraph exceeds 1024 vertices or its left set 8192"
+                                                      : "device error in decomposition";
         return (int)hc.error;
     }
     // k-search jobs: a valid root with |C2| = n - hop owns |C2| + 1 independent jobs
@@ -390,10 +491,13 @@ static int search_impl(kplex_prepared* h, kplex_result* out, kplex_result* per_g
     const int warps_per_block = 8;
     // tuning knobs (environment): blocks per SM the kernel is compiled for (2 or 3) and
     // how many nodes a warp processes on one root before copying its A to shared memory
+    // (params first; the environment variables only fill in defaults)
     const char* eb = getenv("KPLEX_BLOCKS_PER_SM");
-    const int minb = (eb && atoi(eb) == 3) ? 3 : 2;   // measured: 2 blocks x 128 registers beats 3 x 80 + spills
+    int minb = P.blocks_per_sm ? (int)P.blocks_per_sm : (eb ? atoi(eb) : 2);
+    minb = minb == 3 ? 3 : 2;   // measured: 2 blocks x 128 registers beats 3 x 80 + spills
     const char* es = getenv("KPLEX_STAGE_AFTER");
-    sp.stage_after = es ? (uint32_t)atoi(es) : 8u;
+    const int stage_after = P.stage_after ? P.stage_after : (es ? atoi(es) : 8);
+    sp.stage_after = stage_after > 0 ? (uint32_t)stage_after : 0u;
     auto kfn = minb == 2 ? search_kernel_2 : search_kernel_3;
     // stage adjacency matrices in shared memory when minb 8-warp blocks still fit on an SM
     int per_sm = 0;
@@ -402,12 +506,11 @@ static int search_impl(kplex_prepared* h, kplex_result* out, kplex_result* per_g
         sp.a_words = stage ? ((hc.max_nw + 3u) & ~3u) : 0u;
         smem_bytes = (size_t)(ks_slot_words_host(nmax) + warps_per_block * bnb_smem_words_host(nmax, sp.slot_words, sp.a_words)) * 4;
         if (smem_bytes > 227 * 1024) continue;
-        CK(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes));
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, warps_per_block * 32, smem_bytes));
         if (per_sm >= minb || !stage) break;
     }
     per_sm = std::max(per_sm, 1);
-    const uint32_t blocks = (uint32_t)d->sms * (uint32_t)per_sm;
+    const uint32_t blocks = std::max<uint32_t>(1u, (uint32_t)d->sms * (uint32_t)per_sm / std::max<uint32_t>(grid_div, 1u));
     const uint32_t nwarps = blocks * warps_per_block;
     sp.nwarps = nwarps;
     sp.stack_depth = nmax + 2;
@@ -417,9 +520,11 @@ static int search_impl(kplex_prepared* h, kplex_result* out, kplex_result* per_g
     sp.pause_at = (unsigned long long)std::max<long long>(pause, 1);
     if ((rc = d->stacks.ensure((size_t)nwarps * sp.stack_depth * sp.slot_words * 4))) return rc;
     sp.stacks = d->stacks.as<uint32_t>();
+    unsigned long long scap_used = 0;
     if (P.flags & KPLEX_FLAG_SPILL_HOST) {
         // spill ring: control and sequence words in HBM, records in mapped pinned host memory
         const unsigned long long scap = std::min<unsigned long long>(4 * cap, 1ull << 24);
+        scap_used = scap;
         if ((rc = d->spill_ctl.ensure(sizeof(Pool)))) return rc;
         if ((rc = d->spill_seq.ensure((size_t)scap * 4))) return rc;
         if ((rc = d->spill_data.ensure((size_t)scap * sp.slot_words * 4))) return rc;
@@ -452,15 +557,15 @@ static int search_impl(kplex_prepared* h, kplex_result* out, kplex_result* per_g
     cudaEventDestroy(e1);
     cudaEventDestroy(ka);
     cudaEventDestroy(kb);
-    const uint32_t pauses = hc.ks_paused;
     if (!hc.error && hp.head != hp.tail) { hc.error = KPLEX_ERR_TIMEOUT; g_last_error = "branch warps gave up with records left in the pool"; }
     if (per_graph) {
         const size_t G = h->ngraphs;
         std::vector<unsigned long long> gc(G), gh(G);
         std::vector<unsigned int> gv(G);
-        CK(cudaMemcpy(gc.data(), sp.gcount, G * 8, cudaMemcpyDeviceToHost));
-        CK(cudaMemcpy(gh.data(), sp.ghash, G * 8, cudaMemcpyDeviceToHost));
-        CK(cudaMemcpy(gv.data(), sp.gvalid, G * 4, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpyAsync(gc.data(), sp.gcount, G * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(gh.data(), sp.ghash, G * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(gv.data(), sp.gvalid, G * 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
         for (size_t g = 0; g < G; ++g) {
             kplex_result& r = per_graph[g];
             memset(&r, 0, sizeof r);
@@ -469,34 +574,28 @@ static int search_impl(kplex_prepared* h, kplex_result* out, kplex_result* per_g
             r.status = (int)hc.error;
         }
     }
-    if (out) {
-        out->count = hc.count;
-        out->hash = hc.hash;
-        out->valid_roots = hc.valid_roots;
-        out->tasks = hc.tasks;
-        out->nodes = hc.nodes;
-        out->pn = h->pn;
-        out->pm = h->pm;
-        out->max_local_n = hc.max_n;
-        out->max_left = hc.max_left;
-        out->pauses = pauses;
-        out->spilled = (uint32_t)std::min<unsigned long long>(hc.spilled, 0xffffffffull);
-        out->ms_preprocess = h->ms_pre;
-        out->ms_device = ms;
-        out->ms_ref_region = h->ms_pre + ms;
-        out->gpu_launches = launches;
-        out->ms_decompose = ms_dec;
-        out->ms_ksearch = ms_ks;
-        out->ms_bnb = ms_bnb;
-        out->bnb_bytes = hc.bnb_bytes;
-        out->roots_bytes = hc.roots_bytes;
-        out->ks_tasks = hc.ks_tasks;
-        out->stage_copies = hc.stage_copies;
-        out->ks_warp_ms = (double)hc.ks_cycles / (1.965e6);   // SM cycles at the 1965 MHz boost clock
-        out->status = (int)hc.error;
+    fill_result(h, hc, ms, ms_dec, ms_bnb, launches, nroots ? nwarps : 0u, out);
+    if (!hc.error && !(P.flags & KPLEX_FLAG_TEST_NO_WAIT)) {   // sizes are now known: later searches replay a graph
+        Replay* r = new Replay();
+        r->ws = d;
+        r->gen = d->generation();
+        r->p = h->p;
+        r->grid_div = grid_div;
+        r->sp = sp;
+        r->dec_warps = dec_warps;
+        r->blocks = blocks;
+        r->nmax = nmax;
+        r->smem = smem_bytes;
+        r->minb3 = (minb == 3);
+        r->cap = cap;
+        r->scap = sp.spill_on ? scap_used : 0;
+        r->launches = launches;
+        h->replay = r;
     }
     return (int)hc.error;
 }
+
+}  // namespace kplex
 
 // ------------------------------------------------------------------ C ABI
 extern "C" {
@@ -538,7 +637,7 @@ const char* kplex_status_string(int s) {
         case KPLEX_ERR_FORMAT: return "malformed graph";
         case KPLEX_ERR_CUDA: return "cuda error";
         case KPLEX_ERR_NOMEM: return "out of memory";
-        case KPLEX_ERR_CAPACITY: return "root subgraph exceeds 1024 vertices";
+        case KPLEX_ERR_CAPACITY: return "root subgraph exceeds 1024 vertices (or its left set 8192)";
         case KPLEX_ERR_TIMEOUT: return "bounded device wait gave up";
         case KPLEX_ERR_NO_DEVICE: return "no usable CUDA device";
         case KPLEX_ERR_INTERNAL: return "internal device check failed";
@@ -623,7 +722,9 @@ int kplex_search(kplex_prepared* h, kplex_result* out) {
     if (!h) return KPLEX_ERR_PARAM;
     std::lock_guard<std::mutex> lk(g_mu);
     auto t0 = std::chrono::steady_clock::now();
-    int rc = search_impl(h, out);
+    DeviceState* dev = nullptr;
+    int rc = device_state(h->device, &dev);
+    if (rc == KPLEX_OK) rc = search_impl(h, &dev->ws, out);
     if (out) { out->status = rc; out->ms_total = ms_since(t0); }
     return rc;
 }
@@ -645,7 +746,9 @@ int kplex_enumerate_csr(const uint32_t* offsets, const uint32_t* neighbors, uint
     int rc = prepare_impl(offsets, neighbors, n, m_directed, p, &h, r);
     if (rc == KPLEX_OK) {
         if (verbose) { printf("Start copying graph to GPU....\n"); printf("Done copying graph to GPU....\n"); }
-        rc = search_impl(h, r);
+        DeviceState* dev = nullptr;
+        rc = device_state(h->device, &dev);
+        if (rc == KPLEX_OK) rc = search_impl(h, &dev->ws, r);
         free_prepared(h);
     }
     r->status = rc;
@@ -670,7 +773,9 @@ int kplex_prepare_batch(const kplex_job* jobs, uint32_t njobs, const kplex_param
         hj[i] = HostJob{jobs[i].offsets, jobs[i].neighbors, jobs[i].n, jobs[i].m_directed, jobs[i].k, jobs[i].q, jobs[i].truss};
     kplex_params p = *common;
     p.flags |= KPLEX_FLAG_QUIET;
-    int rc = prepare_set(hj, &p, h, total);
+    DeviceState* dev = nullptr;
+    int rc = device_state(p.device, &dev);
+    if (rc == KPLEX_OK) rc = prepare_set(hj, &p, &dev->ws, h, total);
     if (total) total->status = rc;
     return rc;
 }
@@ -682,7 +787,9 @@ int kplex_search_batch(kplex_prepared* h, kplex_result* per_job, kplex_result* t
     kplex_result tmp;
     kplex_result* r = total ? total : &tmp;
     memset(r, 0, sizeof(*r));
-    int rc = search_impl(h, r, per_job);
+    DeviceState* dev = nullptr;
+    int rc = device_state(h->device, &dev);
+    if (rc == KPLEX_OK) rc = search_impl(h, &dev->ws, r, per_job);
     r->status = rc;
     r->ms_total = ms_since(t0);
     return rc;
@@ -703,6 +810,64 @@ int kplex_enumerate_batch(const kplex_job* jobs, uint32_t njobs, const kplex_par
     kplex_release(h);
     r->ms_total = ms_since(t0);
     return rc;
+}
+
+int kplex_autotune_batch(const kplex_job* jobs, uint32_t njobs, const kplex_params* common, uint32_t sample,
+                         kplex_params* best, double* best_ms) {
+    if (!jobs || !njobs || !common || !best) return KPLEX_ERR_PARAM;
+    std::lock_guard<std::mutex> lk(g_mu);
+    sample = std::max<uint32_t>(1u, std::min(sample, njobs));
+    std::vector<HostJob> hj;
+    for (uint32_t i = 0; i < sample; ++i) {
+        const kplex_job& j = jobs[(uint64_t)i * njobs / sample];
+        hj.push_back(HostJob{j.offsets, j.neighbors, j.n, j.m_directed, j.k, j.q, j.truss});
+    }
+    DeviceState* dev = nullptr;
+    int rc = device_state(common->device, &dev);
+    if (rc) return rc;
+    kplex_params p = *common;
+    p.flags |= KPLEX_FLAG_QUIET;
+    kplex_prepared* h = nullptr;
+    kplex_result tot{};
+    if ((rc = prepare_set(hj, &p, &dev->ws, &h, &tot))) return rc;
+    struct Cand { uint32_t bps; int32_t stage; uint64_t pool; float thres; };
+    std::vector<Cand> cands;
+    for (uint32_t bps : {2u, 3u})
+        for (int32_t stage : {8, 32, -1})
+            for (uint64_t pool : {1ull << 20, 1ull << 22})
+                for (float th : {0.25f, 0.5f}) cands.push_back(Cand{bps, stage, pool, th});
+    double best_t = 1e300;
+    uint64_t ref_count = 0, ref_hash = 0;
+    bool have_ref = false;
+    for (const Cand& c : cands) {
+        h->p.blocks_per_sm = c.bps;
+        h->p.stage_after = c.stage;
+        h->p.pool_slots = c.pool;
+        h->p.thres = c.thres;
+        double t = 1e300;
+        for (int rep = 0; rep < 2; ++rep) {   // the first run grows the workspace for this shape
+            kplex_result r{};
+            if ((rc = search_impl(h, &dev->ws, &r))) { free_prepared(h); return rc; }
+            if (!have_ref) { ref_count = r.count; ref_hash = r.hash; have_ref = true; }
+            if (r.count != ref_count || r.hash != ref_hash) {
+                free_prepared(h);
+                g_last_error = "autotune candidates disagree on the sample's result";
+                return KPLEX_ERR_INTERNAL;
+            }
+            if (rep == 1) t = r.ms_device;
+        }
+        if (t < best_t) {
+            best_t = t;
+            *best = *common;
+            best->blocks_per_sm = c.bps;
+            best->stage_after = c.stage;
+            best->pool_slots = c.pool;
+            best->thres = c.thres;
+        }
+    }
+    free_prepared(h);
+    if (best_ms) *best_ms = best_t;
+    return KPLEX_OK;
 }
 
 int kplex_enumerate_file(const char* path, const kplex_params* p, kplex_result* out) {

@@ -169,7 +169,7 @@ extern "C" int kplex_search_noalloc(const uint32_t* d_off, const uint32_t* d_adj
     const int warps_per_block = 8;
     sp.a_words = 0;
     const size_t smem_bytes = (size_t)(ks_slot_words_host(nmax) + warps_per_block * bnb_smem_words_host(nmax, sp.slot_words, 0)) * 4;
-    NA_CK(cudaFuncSetAttribute(search_kernel_3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes));
+    NA_CK(cudaFuncSetAttribute(search_kernel_3, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
     int per_sm = 0;
     NA_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, search_kernel_3, warps_per_block * 32, smem_bytes));
     uint32_t blocks = (uint32_t)sms * (uint32_t)std::max(per_sm, 1);

@@ -721,7 +721,7 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
     uint32_t same_root = 0;
     uint32_t acc_graph = 0;
     unsigned long long tot_cnt = 0, tot_hsum = 0;
-    unsigned long long stage_copies = 0, ks_cycles = 0, spilled = 0, refilled = 0;
+    unsigned long long stage_copies = 0, ks_cycles = 0, spilled = 0, refilled = 0, bnb_cycles = 0, idle_cycles = 0;
     WarpWork ww;
     ww.stack = sp.stacks + (uint64_t)warp * sp.stack_depth * SW;
     ww.sbot = ww.stop = 0;
@@ -774,8 +774,10 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
                 ++stage_copies;
             }
             ++ww.nodes;
+            const long long b0 = clock64();
             have = bnb_node(sp, m, R, A, &t, ww);
             __syncwarp();
+            bnb_cycles += (unsigned long long)(clock64() - b0);
             if (!have && ww.stop == ww.sbot) {
                 ww.stop = ww.sbot = 0;
                 if (counted) { if (l == 0) atomicSub(&sp.ctr->busy, 1u); counted = false; }
@@ -882,6 +884,7 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
             }
         }
         // ---------------- idle: exit when nothing is left anywhere
+        const long long i0 = clock64();
         int done = 0;
         if (l == 0) {
             __threadfence();
@@ -900,6 +903,7 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
             idle = 0;
         }
         __nanosleep(idle < 64 ? 100 : 1000);
+        idle_cycles += (unsigned long long)(clock64() - i0);
     }
     if (l == 0) {
         if (ww.cnt || ww.hsum) { atomicAdd(&sp.gcount[acc_graph], ww.cnt); atomicAdd(&sp.ghash[acc_graph], ww.hsum); }
@@ -914,6 +918,8 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
         atomicAdd(&sp.ctr->ks_cycles, ks_cycles);
         atomicAdd(&sp.ctr->spilled, spilled);
         atomicAdd(&sp.ctr->refilled, refilled);
+        atomicAdd(&sp.ctr->bnb_cycles, bnb_cycles);
+        atomicAdd(&sp.ctr->idle_cycles, idle_cycles);
     }
 }
 

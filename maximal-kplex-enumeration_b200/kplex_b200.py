@@ -31,7 +31,8 @@ class KplexError(RuntimeError):
 class Params(ctypes.Structure):
     _fields_ = [("k", ctypes.c_int), ("q", ctypes.c_int), ("thres", ctypes.c_float), ("truss", ctypes.c_int),
                 ("flags", ctypes.c_uint32), ("device", ctypes.c_int), ("pool_slots", ctypes.c_uint64),
-                ("omp_threads", ctypes.c_uint32), ("shard_index", ctypes.c_uint32), ("shard_count", ctypes.c_uint32)]
+                ("omp_threads", ctypes.c_uint32), ("shard_index", ctypes.c_uint32), ("shard_count", ctypes.c_uint32),
+                ("blocks_per_sm", ctypes.c_uint32), ("stage_after", ctypes.c_int32)]
 
 
 class Result(ctypes.Structure):
@@ -42,7 +43,8 @@ class Result(ctypes.Structure):
                 ("ms_ref_region", ctypes.c_double), ("ms_total", ctypes.c_double), ("status", ctypes.c_int),
                 ("gpu_launches", ctypes.c_uint32), ("ms_decompose", ctypes.c_double), ("ms_ksearch", ctypes.c_double),
                 ("ms_bnb", ctypes.c_double), ("bnb_bytes", ctypes.c_uint64), ("roots_bytes", ctypes.c_uint64),
-                ("ks_tasks", ctypes.c_uint64), ("stage_copies", ctypes.c_uint64), ("ks_warp_ms", ctypes.c_double)]
+                ("ks_tasks", ctypes.c_uint64), ("stage_copies", ctypes.c_uint64), ("ks_warp_ms", ctypes.c_double),
+                ("bnb_warp_ms", ctypes.c_double), ("idle_warp_ms", ctypes.c_double), ("search_warps", ctypes.c_uint32)]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -64,6 +66,31 @@ class GenSpec(ctypes.Structure):
                 ("exponent", ctypes.c_double), ("max_degree", ctypes.c_uint32), ("groups", ctypes.c_uint32),
                 ("group_min", ctypes.c_uint32), ("group_max", ctypes.c_uint32),
                 ("density_min", ctypes.c_double), ("density_max", ctypes.c_double)]
+
+
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("slots", ctypes.c_uint32), ("max_batch", ctypes.c_uint32),
+                ("mem_budget", ctypes.c_uint64), ("split_grid", ctypes.c_uint32), ("thres", ctypes.c_float),
+                ("flags", ctypes.c_uint32), ("pool_slots", ctypes.c_uint64)]
+
+
+class Completion(ctypes.Structure):
+    _fields_ = [("tag", ctypes.c_uint64), ("status", ctypes.c_int), ("batch_size", ctypes.c_uint32),
+                ("count", ctypes.c_uint64), ("hash", ctypes.c_uint64), ("valid_roots", ctypes.c_uint64),
+                ("pn", ctypes.c_uint32), ("slot", ctypes.c_uint32), ("ms_queue", ctypes.c_double),
+                ("ms_service", ctypes.c_double), ("ms_latency", ctypes.c_double)]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64), ("rejected", ctypes.c_uint64),
+                ("launches", ctypes.c_uint64), ("device_bytes", ctypes.c_uint64), ("peak_device_bytes", ctypes.c_uint64),
+                ("max_concurrent", ctypes.c_uint32), ("max_batch_seen", ctypes.c_uint32)]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
 
 
 # The benchmark workloads (seeded synthetic stand-ins for the reference's inputs).
@@ -114,6 +141,15 @@ def lib() -> ctypes.CDLL:
         L.kplex_prepare_batch.argtypes = [ctypes.POINTER(Job), ctypes.c_uint32, ctypes.POINTER(Params),
                                           ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(Result)]
         L.kplex_search_batch.argtypes = [ctypes.c_void_p, ctypes.POINTER(Result), ctypes.POINTER(Result)]
+        L.kplex_autotune_batch.argtypes = [ctypes.POINTER(Job), ctypes.c_uint32, ctypes.POINTER(Params), ctypes.c_uint32,
+                                           ctypes.POINTER(Params), ctypes.POINTER(ctypes.c_double)]
+        L.kplex_server_create.argtypes = [ctypes.POINTER(ServerConfig), ctypes.POINTER(ctypes.c_void_p)]
+        L.kplex_server_submit.argtypes = [ctypes.c_void_p, ctypes.POINTER(Job), ctypes.c_uint64]
+        L.kplex_server_poll.argtypes = [ctypes.c_void_p, ctypes.POINTER(Completion), ctypes.c_uint32, ctypes.c_int]
+        L.kplex_server_drain.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.kplex_server_stats_get.argtypes = [ctypes.c_void_p, ctypes.POINTER(ServerStats)]
+        L.kplex_server_destroy.argtypes = [ctypes.c_void_p]
+        L.kplex_server_destroy.restype = None
         _lib = L
     return _lib
 
@@ -172,8 +208,10 @@ def workload_graph(name: str):
 
 
 def make_params(k: int, q: int, thres: float = 0.25, truss: int = 0, flags: int = FLAG_QUIET, device: int = 0,
-                pool_slots: int = 0, omp_threads: int = 0, shard_index: int = 0, shard_count: int = 0) -> Params:
-    return Params(k, q, thres, truss, flags, device, pool_slots, omp_threads, shard_index, shard_count)
+                pool_slots: int = 0, omp_threads: int = 0, shard_index: int = 0, shard_count: int = 0,
+                blocks_per_sm: int = 0, stage_after: int = 0) -> Params:
+    return Params(k, q, thres, truss, flags, device, pool_slots, omp_threads, shard_index, shard_count,
+                  blocks_per_sm, stage_after)
 
 
 def enumerate_csr(off: np.ndarray, adj: np.ndarray, k: int, q: int, thres: float = 0.25, truss: int = 0,
@@ -253,11 +291,13 @@ def preprocess(off: np.ndarray, adj: np.ndarray, k: int, q: int, truss: int = 0,
             "orig": o_orig[:pn]}
 
 
-def batch_workload(count: int = 4096, seed: int = 4):
+def batch_workload(count: int = 4096, seed: int = 4, min_q_k4: int = 0):
     """The batched workload: `count` independent seeded graphs.  Per graph: n log-uniform
     in [64, 2048], Chung-Lu mean degree U[8, 24] with exponent 2.3, 1-8 planted groups
     of 10-30 vertices at density U[0.85, 0.95], k uniform in {2, 3, 4}, q uniform in [8, 20].
-    Returns a list of (offsets, neighbors, k, q)."""
+    min_q_k4 > 0 raises q to at least that value on the k = 4 graphs (the same graphs
+    and draws otherwise): with q < 12 some k = 4 graphs hold hundreds of millions of
+    maximal 4-plexes each.  Returns a list of (offsets, neighbors, k, q)."""
     rng = np.random.default_rng(seed)
     out = []
     for i in range(count):
@@ -271,6 +311,8 @@ def batch_workload(count: int = 4096, seed: int = 4):
         off, adj = generate(spec)
         k = int(rng.integers(2, 5))
         q = int(rng.integers(8, 21))
+        if k == 4 and min_q_k4:
+            q = max(q, min_q_k4)
         out.append((off, adj, k, q))
     return out
 
@@ -307,10 +349,10 @@ def _jobs(graphs, truss=0):
 
 
 def enumerate_batch(graphs, thres: float = 0.25, truss: int = 0, flags: int = FLAG_QUIET, device: int = 0,
-                    pool_slots: int = 0):
+                    pool_slots: int = 0, blocks_per_sm: int = 0, stage_after: int = 0):
     """graphs: list of (offsets, neighbors, k, q).  Returns (per-graph results, totals)."""
     jobs, keep = _jobs(graphs, truss)
-    p = make_params(2, 3, thres, 0, flags, device, pool_slots)
+    p = make_params(2, 3, thres, 0, flags, device, pool_slots, blocks_per_sm=blocks_per_sm, stage_after=stage_after)
     per = (Result * len(graphs))()
     tot = Result()
     rc = lib().kplex_enumerate_batch(jobs, len(graphs), ctypes.byref(p), per, ctypes.byref(tot))
@@ -320,9 +362,9 @@ def enumerate_batch(graphs, thres: float = 0.25, truss: int = 0, flags: int = FL
 
 
 def prepare_batch(graphs, thres: float = 0.25, truss: int = 0, flags: int = FLAG_QUIET, device: int = 0,
-                  pool_slots: int = 0) -> PreparedBatch:
+                  pool_slots: int = 0, blocks_per_sm: int = 0, stage_after: int = 0) -> PreparedBatch:
     jobs, keep = _jobs(graphs, truss)
-    p = make_params(2, 3, thres, 0, flags, device, pool_slots)
+    p = make_params(2, 3, thres, 0, flags, device, pool_slots, blocks_per_sm=blocks_per_sm, stage_after=stage_after)
     h = ctypes.c_void_p()
     tot = Result()
     rc = lib().kplex_prepare_batch(jobs, len(graphs), ctypes.byref(p), ctypes.byref(h), ctypes.byref(tot))
@@ -331,5 +373,74 @@ def prepare_batch(graphs, thres: float = 0.25, truss: int = 0, flags: int = FLAG
     return PreparedBatch(h, len(graphs), tot.as_dict())
 
 
+def autotune_batch(graphs, sample: int = 256, thres: float = 0.25, truss: int = 0, flags: int = FLAG_QUIET,
+                   device: int = 0) -> tuple[dict, float]:
+    """Schedule chosen by kplex_autotune_batch on a sample of the batch: returns
+    (tuned params as a dict for enumerate_batch/prepare_batch, sample device ms)."""
+    jobs, keep = _jobs(graphs, truss)
+    p = make_params(2, 3, thres, 0, flags, device)
+    best = Params()
+    ms = ctypes.c_double()
+    rc = lib().kplex_autotune_batch(jobs, len(graphs), ctypes.byref(p), sample, ctypes.byref(best), ctypes.byref(ms))
+    if rc:
+        raise _err(rc)
+    return {"thres": best.thres, "pool_slots": best.pool_slots, "blocks_per_sm": best.blocks_per_sm,
+            "stage_after": best.stage_after}, ms.value
+
+
 def device_ok(device: int = 0) -> bool:
     return bool(lib().kplex_device_ok(device))
+
+
+class Server:
+    """Continuous-batching request server (kplex_server_* in include/kplex.h).
+
+    submit() copies the graph and returns at once; completions arrive through
+    poll() as dicts with the request's tag, count, hash and its queue, service
+    and end-to-end latencies in ms."""
+
+    def __init__(self, device: int = 0, slots: int = 2, max_batch: int = 1024, mem_budget: int = 16 << 30,
+                 split_grid: bool = False, thres: float = 0.25, flags: int = FLAG_QUIET, pool_slots: int = 0):
+        cfg = ServerConfig(device, slots, max_batch, mem_budget, 1 if split_grid else 0, thres, flags, pool_slots)
+        h = ctypes.c_void_p()
+        rc = lib().kplex_server_create(ctypes.byref(cfg), ctypes.byref(h))
+        if rc:
+            raise _err(rc)
+        self.handle = h
+
+    def submit(self, off: np.ndarray, adj: np.ndarray, k: int, q: int, truss: int = 0, tag: int = 0) -> None:
+        off = np.ascontiguousarray(off, dtype=np.uint32)
+        adj = np.ascontiguousarray(adj, dtype=np.uint32) if len(adj) else np.zeros(1, np.uint32)
+        m = int(off[-1])
+        job = Job(_u32p(off), _u32p(adj), len(off) - 1, m, k, q, truss)
+        rc = lib().kplex_server_submit(self.handle, ctypes.byref(job), tag)
+        if rc:
+            raise _err(rc)
+
+    def poll(self, max_items: int = 256, timeout_ms: int = 0) -> list[dict]:
+        buf = (Completion * max_items)()
+        n = lib().kplex_server_poll(self.handle, buf, max_items, timeout_ms)
+        if n < 0:
+            raise _err(-n)
+        return [buf[i].as_dict() for i in range(n)]
+
+    def drain(self, timeout_ms: int = -1) -> None:
+        rc = lib().kplex_server_drain(self.handle, timeout_ms)
+        if rc:
+            raise _err(rc)
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        lib().kplex_server_stats_get(self.handle, ctypes.byref(st))
+        return st.as_dict()
+
+    def close(self) -> None:
+        if self.handle:
+            lib().kplex_server_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

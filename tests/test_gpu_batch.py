@@ -33,3 +33,35 @@ def test_batch_reuse_and_mixed_sizes(kp, orc):
     assert a_per[0]["count"] == 871
     o = orc.enumerate_csr(small[0], small[1], 3, 9)
     assert (a_per[-1]["count"], a_per[-1]["hash"]) == (o["count"], o["hash"])
+
+
+def test_repeat_searches_replay_a_captured_graph(kp):
+    """The second and later searches of a prepared set replay a CUDA graph; results
+    stay identical, also after another set grows the shared workspace in between."""
+    graphs = kp.batch_workload(count=32, seed=21)
+    prep = kp.prepare_batch(graphs)
+    try:
+        runs = [prep.search() for _ in range(3)]
+        big = kp.workload_graph("small")
+        other = kp.prepare(big[0], big[1], 3, 9, pool_slots=1 << 23)   # different pool size: buffers move
+        try:
+            other.search()
+        finally:
+            other.release()
+        runs.append(prep.search())
+        runs.append(prep.search())
+    finally:
+        prep.release()
+    first = [(r["count"], r["hash"], r["valid_roots"]) for r in runs[0][0]]
+    for per, tot in runs[1:]:
+        assert [(r["count"], r["hash"], r["valid_roots"]) for r in per] == first
+        assert tot["status"] == 0 and tot["ms_bnb"] > 0 and tot["ms_device"] >= tot["ms_bnb"]
+
+
+def test_autotuned_schedule_same_results(kp):
+    graphs = kp.batch_workload(count=64, seed=22)
+    tuned, ms = kp.autotune_batch(graphs, sample=16)
+    assert ms > 0 and tuned["blocks_per_sm"] in (2, 3)
+    a, _ = kp.enumerate_batch(graphs)
+    b, _ = kp.enumerate_batch(graphs, **tuned)
+    assert [(r["count"], r["hash"]) for r in a] == [(r["count"], r["hash"]) for r in b]
