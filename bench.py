@@ -46,6 +46,11 @@ def load_workload(name: str):
         return off, adj, dict(workload=f"{name}-shaped synthetic" if name != "small" else "small synthetic",
                               seed=w["spec"]["seed"], n=int(len(off) - 1), m_directed=int(len(adj)),
                               k=w["k"], q=w["q"], t=w["thres"], truss=w["truss"])
+    if name.startswith("batch:"):   # graph i of the batched workload, alone
+        i = int(name.split(":")[1])
+        off, adj, k, q = kp.batch_graph(i, 4)
+        return off, adj, dict(workload=f"batched-workload graph {i} (seed 4)", n=int(len(off) - 1),
+                              m_directed=int(len(adj)), k=k, q=q, t=0.25, truss=0)
     # a real .bin graph: name = path:k:q:truss
     path, k, q, tr = name.split(":")
     off, adj = kp.load_bin(path)
@@ -428,11 +433,13 @@ def main():
     # end to end through the public C ABI from host CSR arrays (rank's shard)
     e2e_ms = []
     e2e_count = 0
+    e2e_parts = {}
     for _ in range(args.e2e_steps):
         r = kp.enumerate_csr(off, adj, cfg["k"], cfg["q"], cfg["t"], cfg["truss"], device=local,
                              shard_index=shard_index, shard_count=shard_count)
         e2e_ms.append(r["ms_total"])
         e2e_count = r["count"]
+        e2e_parts = {"ms_preprocess": r["ms_preprocess"], "ms_device": r["ms_device"], "ms_total": r["ms_total"]}
     if world > 1:
         e = torch.tensor([max(e2e_ms)], dtype=torch.float64, device=f"cuda:{local}")
         dist.all_reduce(e, op=dist.ReduceOp.MAX)
@@ -469,7 +476,7 @@ def main():
                      "traffic": traffic, "bytes_per_launch": bnb_bytes / max(bnb_launches, 1),
                      "ms_per_launch": bnb_ms / max(bnb_launches, 1)},
         "e2e": {"value": e2e_total / (e2e_max / 1e3) if e2e_max > 0 else 0.0, "unit": UNIT,
-                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 512, "ms_per_step": e2e_max},
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 512, "ms_per_step": e2e_max, "parts": e2e_parts},
         "gpu_launches": launches,
         "device_counters": {x: res[-1][x] for x in ("tasks", "ks_tasks", "nodes", "valid_roots", "max_local_n",
                                                     "max_left", "pauses", "stage_copies", "roots_bytes", "search_warps")},

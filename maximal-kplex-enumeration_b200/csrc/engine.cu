@@ -34,7 +34,7 @@ __global__ void search_kernel_2(SearchParams sp, uint32_t nmax);
 __global__ void job_prefix_kernel(const RootDesc* roots, uint32_t nroots, uint32_t* job_base);
 uint64_t decomp_scratch_words_host(uint32_t pn);
 uint32_t bnb_smem_words_host(uint32_t nmax, uint32_t slot_words, uint32_t a_words);
-uint32_t ks_slot_words_host(uint32_t nmax);
+uint32_t ks_slot_words_host(uint32_t nmax, uint32_t slot_words);
 
 // ------------------------------------------------------------------ small kernels
 __global__ void init_decomp_scratch(uint32_t* scratch, uint64_t words_per_warp, uint32_t pn, uint32_t nwarps) {
@@ -504,7 +504,7 @@ int search_impl(kplex_prepared* h, Workspace* d, kplex_result* out, kplex_result
     size_t smem_bytes = 0;
     for (int stage = sp.stage_after ? 1 : 0; stage >= 0; --stage) {
         sp.a_words = stage ? ((hc.max_nw + 3u) & ~3u) : 0u;
-        smem_bytes = (size_t)(ks_slot_words_host(nmax) + warps_per_block * bnb_smem_words_host(nmax, sp.slot_words, sp.a_words)) * 4;
+        smem_bytes = (size_t)(ks_slot_words_host(nmax, sp.slot_words) + warps_per_block * bnb_smem_words_host(nmax, sp.slot_words, sp.a_words)) * 4;
         if (smem_bytes > 227 * 1024) continue;
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, warps_per_block * 32, smem_bytes));
         if (per_sm >= minb || !stage) break;

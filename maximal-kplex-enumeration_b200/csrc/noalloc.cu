@@ -45,7 +45,7 @@ __global__ void init_pool(uint32_t* seq, unsigned long long cap, Pool* pool);
 __global__ void job_prefix_kernel(const RootDesc* roots, uint32_t nroots, uint32_t* job_base);
 uint64_t decomp_scratch_words_host(uint32_t pn);
 uint32_t bnb_smem_words_host(uint32_t nmax, uint32_t slot_words, uint32_t a_words);
-uint32_t ks_slot_words_host(uint32_t nmax);
+uint32_t ks_slot_words_host(uint32_t nmax, uint32_t slot_words);
 void set_last_error(const std::string& msg);
 
 namespace {
@@ -168,7 +168,7 @@ extern "C" int kplex_search_noalloc(const uint32_t* d_off, const uint32_t* d_adj
     size_t o2 = align_up(arena_off + (size_t)hc.arena_top * 4, 256);
     const int warps_per_block = 8;
     sp.a_words = 0;
-    const size_t smem_bytes = (size_t)(ks_slot_words_host(nmax) + warps_per_block * bnb_smem_words_host(nmax, sp.slot_words, 0)) * 4;
+    const size_t smem_bytes = (size_t)(ks_slot_words_host(nmax, sp.slot_words) + warps_per_block * bnb_smem_words_host(nmax, sp.slot_words, 0)) * 4;
     NA_CK(cudaFuncSetAttribute(search_kernel_3, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
     int per_sm = 0;
     NA_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, search_kernel_3, warps_per_block * 32, smem_bytes));

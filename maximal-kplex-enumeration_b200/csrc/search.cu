@@ -706,6 +706,89 @@ __device__ __forceinline__ void load_record(const uint32_t* src, uint32_t Wt, No
     }
 }
 
+// ---------------------------------------------------------------- block queue
+// A small LIFO of task records in shared memory, shared by the warps of one
+// block.  A warp that holds stacked work hands its oldest record to an idle
+// warp of its own block through it, and a producer hands new tasks to it while
+// its block has idle warps, with shared-memory atomics only.  The global pool
+// is used when the block has no idle warp, and only one warp per block polls
+// the global pool at a time, so that an almost empty pool is not hammered by
+// every idle warp of the device.  Each record in a block queue holds one unit
+// of the global busy count (taken over by the warp that pops it), so the
+// termination test never sees a record there as finished work.
+constexpr uint32_t BQ_RECORDS = 8;
+constexpr uint32_t BQ_HDR = 8;   // lock, count, idle warps, poller token, pad
+
+__host__ __device__ inline uint32_t bq_words(uint32_t slot_words) {
+    return BQ_HDR + ((BQ_RECORDS * slot_words + 3u) & ~3u);
+}
+
+struct BlockQueue {
+    uint32_t* w;
+    uint32_t SW;
+    __device__ int* lock() const { return reinterpret_cast<int*>(w); }
+    __device__ uint32_t* count() const { return w + 1; }
+    __device__ uint32_t* idle() const { return w + 2; }
+    __device__ int* poller() const { return reinterpret_cast<int*>(w + 3); }
+    __device__ uint32_t* rec(uint32_t i) const { return w + BQ_HDR + i * SW; }
+    __device__ uint32_t n() const { return *(volatile uint32_t*)count(); }
+    __device__ uint32_t idle_warps() const { return *(volatile uint32_t*)idle(); }
+};
+
+// lane 0 only; a bounded spin (the lock is held for one record copy)
+__device__ __forceinline__ bool bq_lock(const BlockQueue& q) {
+    for (int i = 0; i < 1 << 14; ++i) {
+        if (atomicCAS(q.lock(), 0, 1) == 0) { __threadfence_block(); return true; }
+        __nanosleep(32);
+    }
+    return false;
+}
+__device__ __forceinline__ void bq_unlock(const BlockQueue& q) {
+    __threadfence_block();
+    atomicExch(q.lock(), 0);
+}
+
+// Pushes one record (word(i) for i < SW) if the queue has room; whole warp.
+template <typename WordFn>
+__device__ bool bq_push(const BlockQueue& q, WordFn word) {
+    const unsigned l = lane_id();
+    int slot = -1;
+    if (l == 0 && q.n() < BQ_RECORDS && bq_lock(q)) {
+        const uint32_t c = q.n();
+        if (c < BQ_RECORDS) slot = (int)c;
+        else bq_unlock(q);
+    }
+    slot = __shfl_sync(FULL, slot, 0);
+    if (slot < 0) return false;
+    uint32_t* dst = q.rec((uint32_t)slot);
+    for (unsigned i = l; i < q.SW; i += 32) dst[i] = word(i);
+    __threadfence_block();
+    __syncwarp();
+    if (l == 0) { *(volatile uint32_t*)q.count() = (uint32_t)slot + 1; bq_unlock(q); }
+    __syncwarp();
+    return true;
+}
+
+// Pops the newest record into dst (shared memory, SW words); whole warp.
+__device__ bool bq_pop(const BlockQueue& q, uint32_t* dst) {
+    const unsigned l = lane_id();
+    int slot = -1;
+    if (l == 0 && q.n() > 0 && bq_lock(q)) {
+        const uint32_t c = q.n();
+        if (c > 0) slot = (int)c - 1;
+        else bq_unlock(q);
+    }
+    slot = __shfl_sync(FULL, slot, 0);
+    if (slot < 0) return false;
+    const uint32_t* src = q.rec((uint32_t)slot);
+    for (unsigned i = l; i < q.SW; i += 32) dst[i] = src[i];
+    __threadfence_block();
+    __syncwarp();
+    if (l == 0) { *(volatile uint32_t*)q.count() = (uint32_t)slot; bq_unlock(q); }
+    __syncwarp();
+    return true;
+}
+
 __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
     extern __shared__ uint4 smem4[];
     uint32_t* smem = reinterpret_cast<uint32_t*>(smem4);
@@ -716,7 +799,10 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
     const bool producer = (wib == 0);
     const KsLayout KL = ks_layout(nmax);
     const KsSlot S{smem, KL};
-    const BnbSmem m = bnb_smem(smem + KL.total + wib * bnb_smem_words(nmax, SW, sp.a_words), nmax, SW);
+    const BlockQueue BQ{smem + KL.total, SW};
+    const BnbSmem m = bnb_smem(smem + KL.total + bq_words(SW) + wib * bnb_smem_words(nmax, SW, sp.a_words), nmax, SW);
+    if (threadIdx.x < BQ_HDR) BQ.w[threadIdx.x] = 0u;
+    __syncthreads();
     const uint32_t* A = nullptr;
     uint32_t same_root = 0;
     uint32_t acc_graph = 0;
@@ -728,8 +814,14 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
     ww.cnt = ww.hsum = ww.tasks = ww.nodes = ww.bb = 0;
     unsigned long long ks_tasks = 0;
     const unsigned long long resume_at = sp.pause_at / 2 > 0 ? sp.pause_at / 2 : 1;
-    bool have = false, counted = false, ks_active = false, paused = false;
-    unsigned long long idle = 0;
+    bool have = false, counted = false, ks_active = false, paused = false, is_idle = false;
+    unsigned long long idle = 0;   // idle iterations counted toward spin_limit
+    unsigned spins = 0;            // idle iterations since the warp last had work (backoff)
+    // a warp that leaves the idle state (lane 0 keeps the block's idle count)
+    auto wake = [&]() {
+        if (is_idle) { if (l == 0) atomicSub(BQ.idle(), 1u); is_idle = false; }
+        spins = 0;
+    };
     Node t{};
     uint32_t cur_root = 0xffffffffu;
     RootView R{};
@@ -744,13 +836,26 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
             __syncwarp();
         }
         if (have) {
-            if (ww.stop - ww.sbot >= 2 && (ww.nodes & 7) == 0) {   // donate the oldest stacked record
+            if (ww.stop - ww.sbot >= 2) {   // donate the oldest stacked record
+                // to an idle warp of this block when there is one, else (every 8
+                // nodes) to the global pool when it runs low
                 int give = 0;
-                if (l == 0) give = pool_size(sp) < sp.low_water;
+                if (l == 0) {
+                    const uint32_t iw = BQ.idle_warps();
+                    if (iw > 0 && BQ.n() < iw) give = 1;
+                    else if ((ww.nodes & 7) == 0 && pool_size(sp) < sp.low_water) give = 2;
+                }
                 give = __shfl_sync(FULL, give, 0);
                 if (give) {
                     const uint32_t* src = ww.stack + (ww.sbot % sp.stack_depth) * SW;
-                    if (pool_push(sp, [&](unsigned i) { return __ldcg(src + i); })) ++ww.sbot;
+                    auto word = [&](unsigned i) { return __ldcg(src + i); };
+                    if (give == 1) {
+                        if (l == 0) atomicAdd(&sp.ctr->busy, 1u);   // the record's unit, taken over by its popper
+                        if (bq_push(BQ, word)) ++ww.sbot;
+                        else if (l == 0) atomicSub(&sp.ctr->busy, 1u);
+                    } else if (pool_push(sp, word)) {
+                        ++ww.sbot;
+                    }
                 }
             }
             if (t.root != cur_root) {
@@ -818,6 +923,7 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
                         const RootDesc rd = sp.roots[lo2];
                         ks_start(sp, S, lo2, (uint32_t)j - __ldg(sp.job_base + lo2), rd);
                         ks_active = true;
+                        wake();
                     }
                 }
                 if (ks_active) {
@@ -839,7 +945,14 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
                             return which == 0 ? m.P[wi] : (which == 1 ? m.NC[wi] : m.NX[wi]);
                         };
                         bool pushed = false;
-                        if (to_host) {   // spill: the record goes to pinned host memory
+                        int local = 0;   // an idle warp of this block takes it directly
+                        if (l == 0) local = BQ.idle_warps() > BQ.n();
+                        if (__shfl_sync(FULL, local, 0)) {
+                            if (l == 0) atomicAdd(&sp.ctr->busy, 1u);
+                            pushed = bq_push(BQ, word);
+                            if (!pushed && l == 0) atomicSub(&sp.ctr->busy, 1u);
+                        }
+                        if (!pushed && to_host) {   // spill: the record goes to pinned host memory
                             pushed = ring_push(sp, spill_ring(sp), word);
                             if (pushed) ++spilled;
                         }
@@ -848,6 +961,7 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
                             t.root = r; t.np = e.np; t.nc = e.nc; t.nx = e.nx;
                             t.Pw = e.Pw; t.Cw = e.Cw; t.Xw = e.Xw;
                             have = true;
+                            wake();
                             if (!counted) { if (l == 0) atomicAdd(&sp.ctr->busy, 1u); counted = true; }
                         }
                     } else {
@@ -861,16 +975,32 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
                 }
             }
         }
-        // ---------------- consumer: take a record from the pool, else refill from the spill ring
+        // ---------------- consumer: this block's queue, else (one warp per block at a
+        // time) the global pool, else refill from the spill ring
+        if (!is_idle) { if (l == 0) atomicAdd(BQ.idle(), 1u); is_idle = true; }
+        if (bq_pop(BQ, m.rec)) {   // takes over the record's busy unit
+            wake();
+            load_record(m.rec, Wt, &t, false);
+            have = true;
+            counted = true;
+            idle = 0;
+            __syncwarp();
+            continue;
+        }
         {
             int which = 0;   // 1: main pool, 2: spill ring
-            if (l == 0) which = pool_size(sp) > 0 ? 1 : (spill_size(sp) > 0 ? 2 : 0);
+            if (l == 0) {
+                which = pool_size(sp) > 0 ? 1 : (spill_size(sp) > 0 ? 2 : 0);
+                if (which && atomicCAS(BQ.poller(), 0, 1) != 0) which = 0;   // another warp of the block polls
+            }
             which = __shfl_sync(FULL, which, 0);
             if (which) {
                 if (l == 0) atomicAdd(&sp.ctr->busy, 1u);
                 __syncwarp();
                 const bool got = which == 1 ? pool_pop(sp, m.rec) : ring_pop(sp, spill_ring(sp), m.rec);
+                if (l == 0) atomicExch(BQ.poller(), 0);
                 if (got) {
+                    wake();
                     if (which == 2) ++refilled;
                     load_record(m.rec, Wt, &t, false);
                     have = true;
@@ -885,7 +1015,7 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
         }
         // ---------------- idle: exit when nothing is left anywhere
         const long long i0 = clock64();
-        int done = 0;
+        int done = 0, others_busy = 0;
         if (l == 0) {
             __threadfence();
             const unsigned nr = *(volatile unsigned*)&sp.ctr->next_root;
@@ -893,18 +1023,25 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
             const unsigned long long ps = pool_size(sp) + spill_size(sp);
             const unsigned b = *(volatile unsigned*)&sp.ctr->busy;
             done = nr >= sp.njobs && live == 0 && ps == 0 && b == 0;
+            others_busy = b > 0 || live > 0;
         }
         done = __shfl_sync(FULL, done, 0);
+        others_busy = __shfl_sync(FULL, others_busy, 0);
         if (done && !ks_active) break;
-        if (++idle > sp.spin_limit) {
+        // waiting while other warps hold work or run k-search ends when they finish
+        // (their loops are bounded); the limit counts waits with nobody working
+        if (!others_busy || ks_active) ++idle;
+        if (idle > sp.spin_limit) {
             if (l == 0) atomicAdd(&sp.ctr->timeouts, 1u);
             if (!ks_active) break;
             paused = false;   // a producer never waits unboundedly for the pool to drain
             idle = 0;
         }
-        __nanosleep(idle < 64 ? 100 : 1000);
+        ++spins;
+        __nanosleep(spins < 32 ? 128 : (spins < 512 ? 512 : 2048));
         idle_cycles += (unsigned long long)(clock64() - i0);
     }
+    wake();
     if (l == 0) {
         if (ww.cnt || ww.hsum) { atomicAdd(&sp.gcount[acc_graph], ww.cnt); atomicAdd(&sp.ghash[acc_graph], ww.hsum); }
         atomicAdd(&sp.ctr->count, tot_cnt + ww.cnt);
@@ -929,6 +1066,6 @@ __global__ void __launch_bounds__(256, 3) search_kernel_3(SearchParams sp, uint3
 __global__ void __launch_bounds__(256, 2) search_kernel_2(SearchParams sp, uint32_t nmax) { search_body(sp, nmax); }
 
 uint32_t bnb_smem_words_host(uint32_t nmax, uint32_t slot_words, uint32_t a_words) { return bnb_smem_words(nmax, slot_words, a_words); }
-uint32_t ks_slot_words_host(uint32_t nmax) { return ks_layout(nmax).total; }
+uint32_t ks_slot_words_host(uint32_t nmax, uint32_t slot_words) { return ks_layout(nmax).total + bq_words(slot_words); }
 
 }  // namespace kplex
