@@ -885,7 +885,7 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
             bnb_cycles += (unsigned long long)(clock64() - b0);
             if (!have && ww.stop == ww.sbot) {
                 ww.stop = ww.sbot = 0;
-                if (counted) { if (l == 0) atomicSub(&sp.ctr->busy, 1u); counted = false; }
+                if (counted) { if (l == 0) { atomicSub(&sp.ctr->holders, 1u); atomicSub(&sp.ctr->busy, 1u); } counted = false; }
             }
             continue;
         }
@@ -962,7 +962,7 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
                             t.Pw = e.Pw; t.Cw = e.Cw; t.Xw = e.Xw;
                             have = true;
                             wake();
-                            if (!counted) { if (l == 0) atomicAdd(&sp.ctr->busy, 1u); counted = true; }
+                            if (!counted) { if (l == 0) { atomicAdd(&sp.ctr->busy, 1u); atomicAdd(&sp.ctr->holders, 1u); } counted = true; }
                         }
                     } else {
                         ks_active = false;
@@ -983,6 +983,7 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
             load_record(m.rec, Wt, &t, false);
             have = true;
             counted = true;
+            if (l == 0) atomicAdd(&sp.ctr->holders, 1u);
             idle = 0;
             __syncwarp();
             continue;
@@ -1005,6 +1006,7 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
                     load_record(m.rec, Wt, &t, false);
                     have = true;
                     counted = true;
+                    if (l == 0) atomicAdd(&sp.ctr->holders, 1u);
                     idle = 0;
                     __syncwarp();
                     continue;
@@ -1023,7 +1025,9 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
             const unsigned long long ps = pool_size(sp) + spill_size(sp);
             const unsigned b = *(volatile unsigned*)&sp.ctr->busy;
             done = nr >= sp.njobs && live == 0 && ps == 0 && b == 0;
-            others_busy = b > 0 || live > 0;
+            // pollers hold a transient busy unit around every pop attempt; holders
+            // counts only warps with work in hand
+            others_busy = *(volatile unsigned*)&sp.ctr->holders > 0 || live > 0;
         }
         done = __shfl_sync(FULL, done, 0);
         others_busy = __shfl_sync(FULL, others_busy, 0);

@@ -39,16 +39,20 @@ __device__ __forceinline__ int warp_excl_scan(int v, int* total) {
 // Lane l holds word l of a bitset (0 beyond its length).  Writes the set
 // bits' indices in ascending order to list[0..) and returns their count.
 __device__ __forceinline__ int bits_to_list(unsigned w, uint16_t* list) {
+    // words are visited in order (only the non-zero ones); within a word every
+    // lane tests one bit, so all 32 lanes stay active however dense the word is
     const unsigned l = lane_id();
-    int tot;
-    int off = warp_excl_scan(__popc(w), &tot);
-    while (w) {
-        const int b = __ffs(w) - 1;
-        list[off++] = (uint16_t)(l * 32 + b);
-        w &= w - 1;
+    unsigned nz = __ballot_sync(FULL, w != 0u);
+    int off = 0;
+    while (nz) {
+        const int j = __ffs(nz) - 1;
+        nz &= nz - 1;
+        const unsigned word = __shfl_sync(FULL, w, j);
+        if ((word >> l) & 1u) list[off + __popc(word & ((1u << l) - 1u))] = (uint16_t)(j * 32 + l);
+        off += __popc(word);
     }
     __syncwarp();
-    return tot;
+    return off;
 }
 
 __device__ __forceinline__ bool test_bit(const uint32_t* bits, unsigned v) { return (bits[v >> 5] >> (v & 31)) & 1u; }
