@@ -195,8 +195,8 @@ def run_batched(args):
     on the autotuned schedule, against one plain launch per graph."""
     import torch
     torch.cuda.set_device(0)
-    graphs = kp.batch_workload(args.batch_count, 4, min_q_k4=0 if args.batch_full else 12)
-    tuned, tune_ms = kp.autotune_batch(graphs, sample=min(256, len(graphs)))
+    graphs = kp.batch_workload(args.batch_count, 4, q_per_k=0 if args.batch_full else 4)
+    tuned, tune_ms = kp.autotune_batch(graphs, sample=min(128, len(graphs)))
     prep = kp.prepare_batch(graphs, **tuned)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda:0")
     for _ in range(args.warmup):
@@ -231,7 +231,7 @@ def run_batched(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
             "data": "synthetic (seeded Chung-Lu + planted dense groups)",
             "config": {"workload": f"{len(graphs)} graphs, seed 4, n log-uniform [64, 2048], k in {{2,3,4}}, q in [8, 20]"
-                                   + ("" if args.batch_full else ", q raised to >= 12 on the k=4 graphs"),
+                                   + ("" if args.batch_full else ", q raised to >= 4k"),
                        "schedule": tuned, "autotune_sample_ms": tune_ms, "l2": "256 MiB flush between steps"},
             "count": count, "exact_vs_plain": exact,
             "e2e": {"value": count / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d,
@@ -255,7 +255,7 @@ def served_requests(rate: float, duration: float, seed: int = 5):
         if t >= duration:
             break
         times.append(t)
-    small = kp.batch_workload(len(times), seed)
+    small = kp.batch_workload(len(times), seed, q_per_k=4)
     epi = DEFAULT_WORKLOAD.split(":")[0]
     big = kp.load_bin(epi) if os.path.exists(epi) else kp.workload_graph("small")
     big_name = "soc-epinions.bin" if os.path.exists(epi) else "small synthetic"
@@ -354,8 +354,8 @@ def main():
                          "served: an open-loop request stream through the server")
     ap.add_argument("--batch-count", type=int, default=4096)
     ap.add_argument("--batch-full", action="store_true",
-                    help="batched: keep q < 12 on the k=4 graphs (about 12 billion plexes, hours of GPU time)")
-    ap.add_argument("--rate", type=float, default=20.0, help="served: requests per second")
+                    help="batched: keep q < 4k (about 12 billion plexes, hours of GPU time)")
+    ap.add_argument("--rate", type=float, default=5.0, help="served: requests per second")
     ap.add_argument("--duration", type=float, default=60.0, help="served: seconds of arrivals")
     ap.add_argument("--slots", type=int, default=2)
     ap.add_argument("--max-batch", type=int, default=256)

@@ -514,7 +514,7 @@ int search_impl(kplex_prepared* h, Workspace* d, kplex_result* out, kplex_result
     const uint32_t nwarps = blocks * warps_per_block;
     sp.nwarps = nwarps;
     sp.stack_depth = nmax + 2;
-    sp.low_water = 2 * nwarps;
+    sp.low_water = nwarps;
     // the reference pauses at MAX_CAP * thres - WARPS (src:2083, 2384): one record of slack per producer
     const long long pause = (long long)std::floor((double)cap * (double)P.thres) - (long long)blocks;
     sp.pause_at = (unsigned long long)std::max<long long>(pause, 1);

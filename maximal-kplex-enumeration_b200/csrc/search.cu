@@ -372,6 +372,22 @@ __device__ __forceinline__ int rowg_popc_covers(const uint32_t* row, const uint3
     return c;
 }
 
+// popcounts of row & m1 and row & m2 in one pass over the row
+__device__ __forceinline__ void rowg_popc2(const uint32_t* row, const uint32_t* m1, const uint32_t* m2, unsigned W,
+                                           int& c1, int& c2) {
+    int a1 = 0, a2 = 0;
+    const uint4* r4 = reinterpret_cast<const uint4*>(row);
+    const uint4* x4 = reinterpret_cast<const uint4*>(m1);
+    const uint4* y4 = reinterpret_cast<const uint4*>(m2);
+    for (unsigned w = 0; w < W / 4; ++w) {
+        const uint4 a = r4[w], x = x4[w], y = y4[w];
+        a1 += __popc(a.x & x.x) + __popc(a.y & x.y) + __popc(a.z & x.z) + __popc(a.w & x.w);
+        a2 += __popc(a.x & y.x) + __popc(a.y & y.y) + __popc(a.z & y.z) + __popc(a.w & y.w);
+    }
+    c1 = a1;
+    c2 = a2;
+}
+
 struct BnbSmem {
     uint32_t* rec;    // slot_words: record being loaded from the pool
     uint32_t* P;      // 32 words each
@@ -417,17 +433,15 @@ __device__ inline BnbSmem bnb_smem(uint32_t* base, uint32_t nmax, uint32_t slot_
 // The reference's warp pivot rule (src:1628-1663, 1669-1697): the shfl_down
 // tree keeps the current pivot unless the other lane's is strictly smaller in
 // neiInG, or equal with a strictly smaller neiInP.
+// The tree's result is the lowest lane holding the smallest (neiInG, neiInP)
+// among lanes with a candidate (lane 0's empty state when none has one), so it
+// is computed here with one hardware min-reduction and a ballot.
 __device__ __forceinline__ void pivot_tree(int& m, int& v, int& p, int& idx) {
-#pragma unroll
-    for (int o = 16; o; o >>= 1) {
-        const int om = __shfl_down_sync(FULL, m, o);
-        const int ov = __shfl_down_sync(FULL, v, o);
-        const int op = __shfl_down_sync(FULL, p, o);
-        const int oi = __shfl_down_sync(FULL, idx, o);
-        if (om < m || (om == m && ov != -1 && p > op)) { m = om; v = ov; p = op; idx = oi; }
-    }
-    m = __shfl_sync(FULL, m, 0); v = __shfl_sync(FULL, v, 0);
-    p = __shfl_sync(FULL, p, 0); idx = __shfl_sync(FULL, idx, 0);
+    const unsigned key = (v != -1) ? (((unsigned)m << 16) | (unsigned)p) : 0xffffffffu;
+    const unsigned best = __reduce_min_sync(FULL, key);
+    const int src = __ffs(__ballot_sync(FULL, key == best)) - 1;
+    m = __shfl_sync(FULL, m, src); v = __shfl_sync(FULL, v, src);
+    p = __shfl_sync(FULL, p, src); idx = __shfl_sync(FULL, idx, src);
 }
 
 // isMaximal_opt / isMaximalPC_opt (src:703-1000): true when no vertex of the
@@ -540,9 +554,10 @@ __device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootVie
     bits_to_list(Cw, m.list + np);
     const int tot = (int)(np + nc);
     for (int i = l; i < tot; i += 32) {
-        const uint32_t* row = A + (uint32_t)m.list[i] * W;
-        m.gv[i] = (uint16_t)rowg_popc(row, m.PC, W);
-        m.pv[i] = (uint16_t)rowg_popc(row, m.P, W);
+        int g, p;
+        rowg_popc2(A + (uint32_t)m.list[i] * W, m.PC, m.P, W, g, p);
+        m.gv[i] = (uint16_t)g;
+        m.pv[i] = (uint16_t)p;
     }
     if (l == 0) ww.bb += (unsigned long long)(tot + 3) * 4ull * W;   // rows + the record's P, C, X
     __syncwarp();
@@ -552,16 +567,18 @@ __device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootVie
         return false;
     }
     // pivot in P: minimum neiInG, ties to the smaller index (src:1592-1620)
-    unsigned long long key = ~0ull;
+    unsigned long long key = ~0ull;   // (neiInG, vertex, neiInP) of this lane's best P member
     for (int i = l; i < (int)np; i += 32) {
         const unsigned long long kk = ((unsigned long long)m.gv[i] << 32) | ((unsigned long long)m.list[i] << 16) | m.pv[i];
         key = kk < key ? kk : key;
     }
-#pragma unroll
-    for (int o = 16; o; o >>= 1) { const unsigned long long ok = __shfl_xor_sync(FULL, key, o); key = ok < key ? ok : key; }
-    const int minP = (int)(key >> 32);
-    const int pp = (int)((key >> 16) & 0xffff);
-    const int ppP = (int)(key & 0xffff);
+    const unsigned kg = (unsigned)(key >> 32);
+    const unsigned gmin = __reduce_min_sync(FULL, kg);
+    const unsigned kv = (kg == gmin) ? (unsigned)(key & 0xffffffffu) : 0xffffffffu;   // vertex << 16 | neiInP
+    const unsigned vmin = __reduce_min_sync(FULL, kv);
+    const int minP = (int)gmin;
+    const int pp = (int)(vmin >> 16);
+    const int ppP = (int)(vmin & 0xffff);
     if (minP + k < max(q, (int)np)) return false;   // src:1624
     int piv, pmin, pval, pidx;
     if (minP + k < tot) {
@@ -837,13 +854,13 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
         }
         if (have) {
             if (ww.stop - ww.sbot >= 2) {   // donate the oldest stacked record
-                // to an idle warp of this block when there is one, else (every 8
+                // to an idle warp of this block when there is one, else (every 16
                 // nodes) to the global pool when it runs low
                 int give = 0;
                 if (l == 0) {
                     const uint32_t iw = BQ.idle_warps();
                     if (iw > 0 && BQ.n() < iw) give = 1;
-                    else if ((ww.nodes & 7) == 0 && pool_size(sp) < sp.low_water) give = 2;
+                    else if ((ww.nodes & 15) == 0 && pool_size(sp) < sp.low_water) give = 2;
                 }
                 give = __shfl_sync(FULL, give, 0);
                 if (give) {

@@ -291,7 +291,7 @@ def preprocess(off: np.ndarray, adj: np.ndarray, k: int, q: int, truss: int = 0,
             "orig": o_orig[:pn]}
 
 
-def _batch_draws(count: int, seed: int, min_q_k4: int = 0):
+def _batch_draws(count: int, seed: int, q_per_k: int = 0):
     rng = np.random.default_rng(seed)
     for i in range(count):
         n = int(round(float(np.exp(rng.uniform(np.log(64), np.log(2048))))))
@@ -303,28 +303,28 @@ def _batch_draws(count: int, seed: int, min_q_k4: int = 0):
                     density_min=0.85, density_max=0.95)
         k = int(rng.integers(2, 5))
         q = int(rng.integers(8, 21))
-        if k == 4 and min_q_k4:
-            q = max(q, min_q_k4)
+        if q_per_k:
+            q = max(q, q_per_k * k)
         yield spec, k, q
 
 
-def batch_graph(index: int, seed: int = 4, min_q_k4: int = 0):
+def batch_graph(index: int, seed: int = 4, q_per_k: int = 0):
     """Graph `index` of batch_workload(seed=seed) alone: (offsets, neighbors, k, q)."""
-    for i, (spec, k, q) in enumerate(_batch_draws(index + 1, seed, min_q_k4)):
+    for i, (spec, k, q) in enumerate(_batch_draws(index + 1, seed, q_per_k)):
         if i == index:
             off, adj = generate(spec)
             return off, adj, k, q
 
 
-def batch_workload(count: int = 4096, seed: int = 4, min_q_k4: int = 0):
+def batch_workload(count: int = 4096, seed: int = 4, q_per_k: int = 0):
     """The batched workload: `count` independent seeded graphs.  Per graph: n log-uniform
     in [64, 2048], Chung-Lu mean degree U[8, 24] with exponent 2.3, 1-8 planted groups
     of 10-30 vertices at density U[0.85, 0.95], k uniform in {2, 3, 4}, q uniform in [8, 20].
-    min_q_k4 > 0 raises q to at least that value on the k = 4 graphs (the same graphs
-    and draws otherwise): with q < 12 some k = 4 graphs hold hundreds of millions of
-    maximal 4-plexes each.  Returns a list of (offsets, neighbors, k, q)."""
+    q_per_k > 0 raises q to at least q_per_k * k (the same graphs and draws
+    otherwise): with small q the dense planted groups hold hundreds of millions
+    of maximal plexes per graph when k = 4 (one holds 586 M at q = 8).  Returns a list of (offsets, neighbors, k, q)."""
     out = []
-    for spec, k, q in _batch_draws(count, seed, min_q_k4):
+    for spec, k, q in _batch_draws(count, seed, q_per_k):
         off, adj = generate(spec)
         out.append((off, adj, k, q))
     return out

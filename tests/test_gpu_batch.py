@@ -59,7 +59,7 @@ def test_repeat_searches_replay_a_captured_graph(kp):
 
 
 def test_autotuned_schedule_same_results(kp):
-    graphs = kp.batch_workload(count=64, seed=22, min_q_k4=12)
+    graphs = kp.batch_workload(count=64, seed=22, q_per_k=4)
     tuned, ms = kp.autotune_batch(graphs, sample=16)
     assert ms > 0 and tuned["blocks_per_sm"] in (2, 3)
     a, _ = kp.enumerate_batch(graphs)
