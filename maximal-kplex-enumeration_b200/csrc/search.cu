@@ -372,6 +372,18 @@ __device__ __forceinline__ int rowg_popc_covers(const uint32_t* row, const uint3
     return c;
 }
 
+// whether every bit of sat is in row
+__device__ __forceinline__ bool rowg_covers(const uint32_t* row, const uint32_t* sat, unsigned W) {
+    uint32_t miss = 0;
+    const uint4* r4 = reinterpret_cast<const uint4*>(row);
+    const uint4* s4 = reinterpret_cast<const uint4*>(sat);
+    for (unsigned w = 0; w < W / 4; ++w) {
+        const uint4 a = r4[w], t = s4[w];
+        miss |= (t.x & ~a.x) | (t.y & ~a.y) | (t.z & ~a.z) | (t.w & ~a.w);
+    }
+    return miss == 0;
+}
+
 // popcounts of row & m1 and row & m2 in one pass over the row
 __device__ __forceinline__ void rowg_popc2(const uint32_t* row, const uint32_t* m1, const uint32_t* m2, unsigned W,
                                            int& c1, int& c2) {
@@ -618,9 +630,7 @@ __device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootVie
             bool ext = false;
             for (int i = l; i < nxl; i += 32) {   // isKplexPC2 src:601-622
                 if ((int)m.gv[tot + i] + k < tot + 1) continue;
-                bool ok;
-                rowg_popc_covers(A + (uint32_t)m.list[tot + i] * W, m.SAT, m.SAT, W, &ok);
-                ext |= ok;
+                ext |= rowg_covers(A + (uint32_t)m.list[tot + i] * W, m.SAT, W);
             }
             if (l == 0) ww.bb += (unsigned long long)nxl * 4ull * W;
             if (__any_sync(FULL, ext)) return false;
@@ -667,9 +677,7 @@ __device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootVie
         if (c == v || !test_bit(m.M2, c)) continue;
         const int pc = (int)m.pv[np + i] + (int)test_bit(m.ROW, c);
         if (pc + k < (int)np1 + 1) continue;
-        bool ok;
-        rowg_popc_covers(A + c * W, m.SAT, m.SAT, W, &ok);
-        if (ok) atomicOr(&m.NC[c >> 5], 1u << (c & 31));
+        if (rowg_covers(A + c * W, m.SAT, W)) atomicOr(&m.NC[c >> 5], 1u << (c & 31));
     }
     if (l == 0) ww.bb += (unsigned long long)nc * 4ull * W;
     __syncwarp();
