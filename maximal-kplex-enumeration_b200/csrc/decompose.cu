@@ -407,7 +407,8 @@ uint64_t decomp_scratch_words_host(uint32_t pn) { return decomp_scratch_words(pn
 
 // k-search job prefix: a valid root with |C2| = n - hop owns |C2| + 1 jobs;
 // job_base[r] = jobs of roots < r, job_base[nroots] = total.  One block.
-__global__ void __launch_bounds__(1024) job_prefix_kernel(const RootDesc* roots, uint32_t nroots, uint32_t* job_base) {
+__global__ void __launch_bounds__(1024) job_prefix_kernel(const RootDesc* roots, uint32_t nroots, uint32_t* job_base,
+                                                                unsigned int* work) {
     __shared__ uint32_t part[1024];
     const uint32_t t = threadIdx.x, T = blockDim.x;
     const uint32_t per = (nroots + T - 1) / T;
@@ -431,7 +432,10 @@ __global__ void __launch_bounds__(1024) job_prefix_kernel(const RootDesc* roots,
         const RootDesc& rd = roots[r];
         run += ((rd.flags & ROOT_VALID) && rd.n) ? rd.n - rd.hop + 1 : 0u;
     }
-    if (t == T - 1) job_base[nroots] = part[T - 1];
+    if (t == T - 1) {
+        job_base[nroots] = part[T - 1];
+        if (work) *work = part[T - 1];   // every job is one outstanding unit of work
+    }
 }
 
 }  // namespace kplex

@@ -31,7 +31,7 @@ namespace kplex {
 __global__ void decompose_kernel(SearchParams sp);
 __global__ void search_kernel_3(SearchParams sp, uint32_t nmax);
 __global__ void search_kernel_2(SearchParams sp, uint32_t nmax);
-__global__ void job_prefix_kernel(const RootDesc* roots, uint32_t nroots, uint32_t* job_base);
+__global__ void job_prefix_kernel(const RootDesc* roots, uint32_t nroots, uint32_t* job_base, unsigned int* work);
 uint64_t decomp_scratch_words_host(uint32_t pn);
 uint32_t bnb_smem_words_host(uint32_t nmax, uint32_t slot_words, uint32_t a_words);
 uint32_t ks_slot_words_host(uint32_t nmax, uint32_t slot_words);
@@ -324,7 +324,7 @@ static int replay_capture(kplex_prepared* h, Replay& r, Workspace* d, bool per_g
         decompose_kernel<<<r.dec_warps / 8, 256, 0, st>>>(sp);
         cudaEventRecordWithFlags(r.ev[2], st, cudaEventRecordExternal);
     }
-    job_prefix_kernel<<<1, 1024, 0, st>>>(sp.roots, h->nroots, d->jobs.as<uint32_t>());
+    job_prefix_kernel<<<1, 1024, 0, st>>>(sp.roots, h->nroots, d->jobs.as<uint32_t>(), &sp.ctr->work);
     init_pool<<<d->sms * 4, 256, 0, st>>>(sp.pool_seq, r.cap, sp.pool);
     if (sp.spill_on) init_pool<<<d->sms * 4, 256, 0, st>>>(sp.spill_seq, r.scap, sp.spill_pool);
     cudaEventRecordWithFlags(r.ev[3], st, cudaEventRecordExternal);
@@ -364,7 +364,7 @@ static int replay_search(kplex_prepared* h, Replay& r, Workspace* d, kplex_resul
     CK(cudaEventElapsedTime(&ms, r.ev[0], r.ev[5]));
     if (h->nroots) CK(cudaEventElapsedTime(&t_dec, r.ev[1], r.ev[2]));
     CK(cudaEventElapsedTime(&t_bnb, r.ev[3], r.ev[4]));
-    if (!hc.error && hp.head != hp.tail) { hc.error = KPLEX_ERR_TIMEOUT; g_last_error = "branch warps gave up with records left in the pool"; }
+    if (!hc.error && (hp.head != hp.tail || hc.work != 0)) { hc.error = KPLEX_ERR_TIMEOUT; g_last_error = "branch warps gave up with work left"; }
     if (hc.error && g_last_error.empty()) g_last_error = "device error in a replayed search";
     if (per_graph) {
         for (size_t g = 0; g < h->ngraphs; ++g) {
@@ -467,7 +467,7 @@ int search_impl(kplex_prepared* h, Workspace* d, kplex_result* out, kplex_result
     // k-search jobs: a valid root with |C2| = n - hop owns |C2| + 1 independent jobs
     if ((rc = d->jobs.ensure(((size_t)nroots + 1) * 4))) return rc;
     sp.job_base = d->jobs.as<uint32_t>();
-    job_prefix_kernel<<<1, 1024, 0, st>>>(sp.roots, nroots, d->jobs.as<uint32_t>());
+    job_prefix_kernel<<<1, 1024, 0, st>>>(sp.roots, nroots, d->jobs.as<uint32_t>(), &sp.ctr->work);
     ++launches;
     uint32_t njobs = 0;
     CK(cudaMemcpyAsync(&njobs, d->jobs.as<uint32_t>() + nroots, 4, cudaMemcpyDeviceToHost, st));
@@ -557,7 +557,7 @@ int search_impl(kplex_prepared* h, Workspace* d, kplex_result* out, kplex_result
     cudaEventDestroy(e1);
     cudaEventDestroy(ka);
     cudaEventDestroy(kb);
-    if (!hc.error && hp.head != hp.tail) { hc.error = KPLEX_ERR_TIMEOUT; g_last_error = "branch warps gave up with records left in the pool"; }
+    if (!hc.error && (hp.head != hp.tail || hc.work != 0)) { hc.error = KPLEX_ERR_TIMEOUT; g_last_error = "branch warps gave up with work left"; }
     if (per_graph) {
         const size_t G = h->ngraphs;
         std::vector<unsigned long long> gc(G), gh(G);

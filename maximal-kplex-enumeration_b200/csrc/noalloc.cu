@@ -42,7 +42,7 @@ __global__ void decompose_kernel(SearchParams sp);
 __global__ void search_kernel_3(SearchParams sp, uint32_t nmax);
 __global__ void init_decomp_scratch(uint32_t* scratch, uint64_t words_per_warp, uint32_t pn, uint32_t nwarps);
 __global__ void init_pool(uint32_t* seq, unsigned long long cap, Pool* pool);
-__global__ void job_prefix_kernel(const RootDesc* roots, uint32_t nroots, uint32_t* job_base);
+__global__ void job_prefix_kernel(const RootDesc* roots, uint32_t nroots, uint32_t* job_base, unsigned int* work);
 uint64_t decomp_scratch_words_host(uint32_t pn);
 uint32_t bnb_smem_words_host(uint32_t nmax, uint32_t slot_words, uint32_t a_words);
 uint32_t ks_slot_words_host(uint32_t nmax, uint32_t slot_words);
@@ -152,7 +152,7 @@ extern "C" int kplex_search_noalloc(const uint32_t* d_off, const uint32_t* d_adj
                                                        : "a root's subgraph exceeds 1024 vertices");
             return out->status = (int)hc.error;
         }
-        job_prefix_kernel<<<1, 1024, 0, st>>>(roots, nroots, job_base);
+        job_prefix_kernel<<<1, 1024, 0, st>>>(roots, nroots, job_base, &ctr->work);
         ++launches;
         uint32_t njobs = 0;
         NA_CK(cudaMemcpyAsync(&njobs, job_base + nroots, 4, cudaMemcpyDeviceToHost, st));

@@ -445,11 +445,14 @@ __device__ inline BnbSmem bnb_smem(uint32_t* base, uint32_t nmax, uint32_t slot_
 // The reference's warp pivot rule (src:1628-1663, 1669-1697): the shfl_down
 // tree keeps the current pivot unless the other lane's is strictly smaller in
 // neiInG, or equal with a strictly smaller neiInP.
-// The tree's result is the lowest lane holding the smallest (neiInG, neiInP)
-// among lanes with a candidate (lane 0's empty state when none has one), so it
-// is computed here with one hardware min-reduction and a ballot.
+// Each step keeps the lower lane's pivot on a tie, so among lanes holding the
+// smallest (neiInG, neiInP) the tree returns the one whose lane index, read
+// with its 5 bits reversed, is smallest (lane 0 before 16 before 8 before 24
+// ...), and lane 0's empty state when no lane has a candidate.  That order is
+// folded into one key for a hardware min-reduction and a ballot.
 __device__ __forceinline__ void pivot_tree(int& m, int& v, int& p, int& idx) {
-    const unsigned key = (v != -1) ? (((unsigned)m << 16) | (unsigned)p) : 0xffffffffu;
+    const unsigned rank = __brev(lane_id()) >> 27;
+    const unsigned key = (v != -1) ? (((unsigned)m << 21) | ((unsigned)p << 5) | rank) : 0xffffffffu;
     const unsigned best = __reduce_min_sync(FULL, key);
     const int src = __ffs(__ballot_sync(FULL, key == best)) - 1;
     m = __shfl_sync(FULL, m, src); v = __shfl_sync(FULL, v, src);
@@ -738,9 +741,15 @@ __device__ __forceinline__ void load_record(const uint32_t* src, uint32_t Wt, No
 // its block has idle warps, with shared-memory atomics only.  The global pool
 // is used when the block has no idle warp, and only one warp per block polls
 // the global pool at a time, so that an almost empty pool is not hammered by
-// every idle warp of the device.  Each record in a block queue holds one unit
-// of the global busy count (taken over by the warp that pops it), so the
-// termination test never sees a record there as finished work.
+// every idle warp of the device.
+//
+// Termination: the counter `work` holds one unit per unclaimed or running
+// k-search job, per record in the pool, a block queue or the spill ring, and
+// per warp holding work.  A unit is added before a record becomes visible and
+// removed (after a fence) only when a job or a warp's work ends; taking a
+// record moves its unit to the taker.  So the count is zero exactly when the
+// search is finished, and no combination of separately read counters can show
+// a finished state while a record is in flight.
 constexpr uint32_t BQ_RECORDS = 8;
 constexpr uint32_t BQ_HDR = 8;   // lock, count, idle warps, poller token, pad
 
@@ -874,13 +883,12 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
                 if (give) {
                     const uint32_t* src = ww.stack + (ww.sbot % sp.stack_depth) * SW;
                     auto word = [&](unsigned i) { return __ldcg(src + i); };
-                    if (give == 1) {
-                        if (l == 0) atomicAdd(&sp.ctr->busy, 1u);   // the record's unit, taken over by its popper
-                        if (bq_push(BQ, word)) ++ww.sbot;
-                        else if (l == 0) atomicSub(&sp.ctr->busy, 1u);
-                    } else if (pool_push(sp, word)) {
-                        ++ww.sbot;
-                    }
+                    // the record becomes a unit of work before it can be seen (and taken)
+                    if (l == 0) { atomicAdd(&sp.ctr->work, 1u); __threadfence(); }
+                    __syncwarp();
+                    const bool ok = (give == 1) ? bq_push(BQ, word) : pool_push(sp, word);
+                    if (ok) ++ww.sbot;
+                    else if (l == 0) atomicSub(&sp.ctr->work, 1u);
                 }
             }
             if (t.root != cur_root) {
@@ -910,7 +918,10 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
             bnb_cycles += (unsigned long long)(clock64() - b0);
             if (!have && ww.stop == ww.sbot) {
                 ww.stop = ww.sbot = 0;
-                if (counted) { if (l == 0) { atomicSub(&sp.ctr->holders, 1u); atomicSub(&sp.ctr->busy, 1u); } counted = false; }
+                if (counted) {   // after this warp's pushes are visible, its unit ends
+                    if (l == 0) { __threadfence(); atomicSub(&sp.ctr->holders, 1u); atomicSub(&sp.ctr->work, 1u); }
+                    counted = false;
+                }
             }
             continue;
         }
@@ -970,13 +981,11 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
                             return which == 0 ? m.P[wi] : (which == 1 ? m.NC[wi] : m.NX[wi]);
                         };
                         bool pushed = false;
+                        if (l == 0) { atomicAdd(&sp.ctr->work, 1u); __threadfence(); }   // the task's unit
+                        __syncwarp();
                         int local = 0;   // an idle warp of this block takes it directly
                         if (l == 0) local = BQ.idle_warps() > BQ.n();
-                        if (__shfl_sync(FULL, local, 0)) {
-                            if (l == 0) atomicAdd(&sp.ctr->busy, 1u);
-                            pushed = bq_push(BQ, word);
-                            if (!pushed && l == 0) atomicSub(&sp.ctr->busy, 1u);
-                        }
+                        if (__shfl_sync(FULL, local, 0)) pushed = bq_push(BQ, word);
                         if (!pushed && to_host) {   // spill: the record goes to pinned host memory
                             pushed = ring_push(sp, spill_ring(sp), word);
                             if (pushed) ++spilled;
@@ -987,12 +996,17 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
                             t.Pw = e.Pw; t.Cw = e.Cw; t.Xw = e.Xw;
                             have = true;
                             wake();
-                            if (!counted) { if (l == 0) { atomicAdd(&sp.ctr->busy, 1u); atomicAdd(&sp.ctr->holders, 1u); } counted = true; }
+                            if (!counted) { if (l == 0) atomicAdd(&sp.ctr->holders, 1u); counted = true; }
                         }
                     } else {
                         ks_active = false;
                         __syncwarp();
-                        if (l == 0) { S.root() = 0xffffffffu; __threadfence(); atomicSub(&sp.ctr->ks_active, 1u); }
+                        if (l == 0) {   // the job's unit ends after its tasks are visible
+                            S.root() = 0xffffffffu;
+                            __threadfence();
+                            atomicSub(&sp.ctr->ks_active, 1u);
+                            atomicSub(&sp.ctr->work, 1u);
+                        }
                         __syncwarp();
                     }
                     idle = 0;
@@ -1003,7 +1017,7 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
         // ---------------- consumer: this block's queue, else (one warp per block at a
         // time) the global pool, else refill from the spill ring
         if (!is_idle) { if (l == 0) atomicAdd(BQ.idle(), 1u); is_idle = true; }
-        if (bq_pop(BQ, m.rec)) {   // takes over the record's busy unit
+        if (bq_pop(BQ, m.rec)) {   // takes over the record's unit of work
             wake();
             load_record(m.rec, Wt, &t, false);
             have = true;
@@ -1021,8 +1035,6 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
             }
             which = __shfl_sync(FULL, which, 0);
             if (which) {
-                if (l == 0) atomicAdd(&sp.ctr->busy, 1u);
-                __syncwarp();
                 const bool got = which == 1 ? pool_pop(sp, m.rec) : ring_pop(sp, spill_ring(sp), m.rec);
                 if (l == 0) atomicExch(BQ.poller(), 0);
                 if (got) {
@@ -1036,7 +1048,6 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
                     __syncwarp();
                     continue;
                 }
-                if (l == 0) atomicSub(&sp.ctr->busy, 1u);
                 __syncwarp();
             }
         }
@@ -1045,13 +1056,10 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
         int done = 0, others_busy = 0;
         if (l == 0) {
             __threadfence();
-            const unsigned nr = *(volatile unsigned*)&sp.ctr->next_root;
+            // one counter covers every place work can be (a unit moves, never
+            // vanishes, when a record is taken), so zero means finished
+            done = atomicAdd(&sp.ctr->work, 0u) == 0u;
             const unsigned live = *(volatile unsigned*)&sp.ctr->ks_active;
-            const unsigned long long ps = pool_size(sp) + spill_size(sp);
-            const unsigned b = *(volatile unsigned*)&sp.ctr->busy;
-            done = nr >= sp.njobs && live == 0 && ps == 0 && b == 0;
-            // pollers hold a transient busy unit around every pop attempt; holders
-            // counts only warps with work in hand
             others_busy = *(volatile unsigned*)&sp.ctr->holders > 0 || live > 0;
         }
         done = __shfl_sync(FULL, done, 0);
