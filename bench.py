@@ -455,12 +455,14 @@ def main():
     peak, peak_kind = measured_peak()
     achieved = (bnb_bytes / (bnb_ms / 1e3)) / 1e9 if bnb_ms > 0 else 0.0
     traffic = None
-    prof = os.path.join(ROOT, "profiles", "bnb_traffic.json")
+    # DRAM bytes per launch of the search kernel from an ncu capture ("key: value" lines)
+    prof = os.path.join(ROOT, "profiles", "search_kernel_traffic.txt")
     if os.path.exists(prof):
         with open(prof) as f:
-            pj = json.load(f)
-        if pj.get("workload") == cfg["workload"]:
-            traffic = pj.get("dram_bytes_per_launch")
+            pj = dict(line.split(":", 1) for line in f if ":" in line and not line.startswith("#"))
+        pj = {k.strip(): v.strip() for k, v in pj.items()}
+        if pj.get("workload") == cfg["workload"] and "dram_bytes_per_launch" in pj:
+            traffic = float(pj["dram_bytes_per_launch"])
 
     line = {
         "metric": METRIC,
