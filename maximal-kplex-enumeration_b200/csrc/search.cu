@@ -414,12 +414,13 @@ struct BnbSmem {
     uint16_t* list;   // nmax
     uint16_t* gv;     // nmax
     uint16_t* pv;     // nmax
+    unsigned long long* CT;   // 16 per-warp counters (lane 0 updates them; kept out of registers)
     uint32_t* A;      // a_words: the current root's adjacency matrix, when it fits
 };
 
 __host__ __device__ inline uint32_t bnb_smem_words(uint32_t nmax, uint32_t slot_words, uint32_t a_words) {
     const uint32_t lists = 3 * ((nmax + 1) / 2);
-    return (((slot_words + 9 * MAX_WORDS + lists) + 3u) & ~3u) + a_words;
+    return (((slot_words + 9 * MAX_WORDS + lists) + 3u) & ~3u) + 32u + a_words;
 }
 
 __device__ inline BnbSmem bnb_smem(uint32_t* base, uint32_t nmax, uint32_t slot_words) {
@@ -438,7 +439,8 @@ __device__ inline BnbSmem bnb_smem(uint32_t* base, uint32_t nmax, uint32_t slot_
     m.list = reinterpret_cast<uint16_t*>(p); p += (nmax + 1) / 2;
     m.gv = reinterpret_cast<uint16_t*>(p); p += (nmax + 1) / 2;
     m.pv = reinterpret_cast<uint16_t*>(p); p += (nmax + 1) / 2;
-    m.A = base + (((slot_words + 9 * MAX_WORDS + 3 * ((nmax + 1) / 2)) + 3u) & ~3u);
+    m.CT = reinterpret_cast<unsigned long long*>(base + (((slot_words + 9 * MAX_WORDS + 3 * ((nmax + 1) / 2)) + 3u) & ~3u));
+    m.A = reinterpret_cast<uint32_t*>(m.CT + 16);
     return m;
 }
 
@@ -546,10 +548,17 @@ struct Node {
     uint32_t Pw, Cw, Xw;   // this lane's word of each bitset
 };
 
+// Counters live in the warp's shared memory (m.CT) and are updated by lane 0.
+enum : int { CT_CNT, CT_HSUM, CT_TASKS, CT_NODES, CT_BB, CT_TOT_CNT, CT_TOT_HSUM, CT_STAGE, CT_KS_CYC, CT_SPILL,
+             CT_REFILL, CT_BNB_CYC, CT_IDLE_CYC, CT_KS_TASKS };
 struct WarpWork {
     uint32_t* stack;
     unsigned long long sbot, stop;
-    unsigned long long cnt, hsum, tasks, nodes, bb;
+    unsigned long long& cnt;
+    unsigned long long& hsum;
+    unsigned long long& tasks;
+    unsigned long long& nodes;
+    unsigned long long& bb;
 };
 
 // One branch-and-bound node (BNB, src:1516-1724).  Returns true when the node
@@ -840,13 +849,11 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
     const uint32_t* A = nullptr;
     uint32_t same_root = 0;
     uint32_t acc_graph = 0;
-    unsigned long long tot_cnt = 0, tot_hsum = 0;
-    unsigned long long stage_copies = 0, ks_cycles = 0, spilled = 0, refilled = 0, bnb_cycles = 0, idle_cycles = 0;
-    WarpWork ww;
-    ww.stack = sp.stacks + (uint64_t)warp * sp.stack_depth * SW;
-    ww.sbot = ww.stop = 0;
-    ww.cnt = ww.hsum = ww.tasks = ww.nodes = ww.bb = 0;
-    unsigned long long ks_tasks = 0;
+    unsigned long long* CT = m.CT;
+    if (l < 16) CT[l] = 0ull;
+    __syncwarp();
+    WarpWork ww{sp.stacks + (uint64_t)warp * sp.stack_depth * SW, 0ull, 0ull,
+                CT[CT_CNT], CT[CT_HSUM], CT[CT_TASKS], CT[CT_NODES], CT[CT_BB]};
     const unsigned long long resume_at = sp.pause_at / 2 > 0 ? sp.pause_at / 2 : 1;
     bool have = false, counted = false, ks_active = false, paused = false, is_idle = false;
     unsigned long long idle = 0;   // idle iterations counted toward spin_limit
@@ -896,8 +903,8 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
                 cur_root = t.root;
                 if (R.graph != acc_graph) {   // results are kept per input graph
                     if (l == 0 && (ww.cnt || ww.hsum)) { atomicAdd(&sp.gcount[acc_graph], ww.cnt); atomicAdd(&sp.ghash[acc_graph], ww.hsum); }
-                    tot_cnt += ww.cnt; tot_hsum += ww.hsum;
-                    ww.cnt = ww.hsum = 0;
+                    if (l == 0) { CT[CT_TOT_CNT] += ww.cnt; CT[CT_TOT_HSUM] += ww.hsum; ww.cnt = ww.hsum = 0; }
+                    __syncwarp();
                     acc_graph = R.graph;
                 }
                 A = R.A;
@@ -909,13 +916,13 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
                 for (uint32_t i = l; i < R.n * R.W / 4; i += 32) dst[i] = __ldg(src + i);
                 __syncwarp();
                 A = m.A;
-                ++stage_copies;
+                if (l == 0) ++CT[CT_STAGE];
             }
-            ++ww.nodes;
+            if (l == 0) ++ww.nodes;
             const long long b0 = clock64();
             have = bnb_node(sp, m, R, A, &t, ww);
             __syncwarp();
-            bnb_cycles += (unsigned long long)(clock64() - b0);
+            if (l == 0) CT[CT_BNB_CYC] += (unsigned long long)(clock64() - b0);
             if (!have && ww.stop == ww.sbot) {
                 ww.stop = ww.sbot = 0;
                 if (counted) {   // after this warp's pushes are visible, its unit ends
@@ -965,9 +972,9 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
                 if (ks_active) {
                     const long long c0 = clock64();
                     const int got = ks_advance(sp, S, &e);
-                    ks_cycles += (unsigned long long)(clock64() - c0);
+                    if (l == 0) CT[CT_KS_CYC] += (unsigned long long)(clock64() - c0);
                     if (got) {
-                        ++ks_tasks;
+                        if (l == 0) ++CT[CT_KS_TASKS];
                         const uint32_t r = S.root();
                         // stage this lane's words in shared memory; the record is hdr | P | C | X
                         m.P[l] = e.Pw; m.NC[l] = e.Cw; m.NX[l] = e.Xw;
@@ -988,7 +995,7 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
                         if (__shfl_sync(FULL, local, 0)) pushed = bq_push(BQ, word);
                         if (!pushed && to_host) {   // spill: the record goes to pinned host memory
                             pushed = ring_push(sp, spill_ring(sp), word);
-                            if (pushed) ++spilled;
+                            if (pushed && l == 0) ++CT[CT_SPILL];
                         }
                         if (!pushed) pushed = pool_push(sp, word);
                         if (!pushed) {   // ring full: keep the task
@@ -1039,7 +1046,7 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
                 if (l == 0) atomicExch(BQ.poller(), 0);
                 if (got) {
                     wake();
-                    if (which == 2) ++refilled;
+                    if (which == 2 && l == 0) ++CT[CT_REFILL];
                     load_record(m.rec, Wt, &t, false);
                     have = true;
                     counted = true;
@@ -1076,24 +1083,24 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
         }
         ++spins;
         __nanosleep(spins < 32 ? 128 : (spins < 512 ? 512 : 2048));
-        idle_cycles += (unsigned long long)(clock64() - i0);
+        if (l == 0) CT[CT_IDLE_CYC] += (unsigned long long)(clock64() - i0);
     }
     wake();
     if (l == 0) {
         if (ww.cnt || ww.hsum) { atomicAdd(&sp.gcount[acc_graph], ww.cnt); atomicAdd(&sp.ghash[acc_graph], ww.hsum); }
-        atomicAdd(&sp.ctr->count, tot_cnt + ww.cnt);
-        atomicAdd(&sp.ctr->hash, tot_hsum + ww.hsum);
-        atomicAdd(&sp.ctr->tasks, ww.tasks + ks_tasks);
-        atomicAdd(&sp.ctr->ks_tasks, ks_tasks);
+        atomicAdd(&sp.ctr->count, CT[CT_TOT_CNT] + ww.cnt);
+        atomicAdd(&sp.ctr->hash, CT[CT_TOT_HSUM] + ww.hsum);
+        atomicAdd(&sp.ctr->tasks, ww.tasks + CT[CT_KS_TASKS]);
+        atomicAdd(&sp.ctr->ks_tasks, CT[CT_KS_TASKS]);
         atomicAdd(&sp.ctr->nodes, ww.nodes);
         atomicAdd(&sp.ctr->bnb_bytes, ww.bb);
         atomicAdd(&sp.ctr->bnb_done, 1u);
-        atomicAdd(&sp.ctr->stage_copies, stage_copies);
-        atomicAdd(&sp.ctr->ks_cycles, ks_cycles);
-        atomicAdd(&sp.ctr->spilled, spilled);
-        atomicAdd(&sp.ctr->refilled, refilled);
-        atomicAdd(&sp.ctr->bnb_cycles, bnb_cycles);
-        atomicAdd(&sp.ctr->idle_cycles, idle_cycles);
+        atomicAdd(&sp.ctr->stage_copies, CT[CT_STAGE]);
+        atomicAdd(&sp.ctr->ks_cycles, CT[CT_KS_CYC]);
+        atomicAdd(&sp.ctr->spilled, CT[CT_SPILL]);
+        atomicAdd(&sp.ctr->refilled, CT[CT_REFILL]);
+        atomicAdd(&sp.ctr->bnb_cycles, CT[CT_BNB_CYC]);
+        atomicAdd(&sp.ctr->idle_cycles, CT[CT_IDLE_CYC]);
     }
 }
 
