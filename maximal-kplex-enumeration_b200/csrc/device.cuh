@@ -81,7 +81,6 @@ struct Counters {
     unsigned int next_root;        // k-search job dispenser
     unsigned int ks_paused;        // k-search warps that stopped at the pause threshold
     unsigned int ks_active;        // k-search slots holding an unfinished root
-    unsigned int busy;             // branch warps holding work (termination detection)
     unsigned int holders;          // warps holding work now (the idle-wait heuristic)
     unsigned int work;             // outstanding work units: unclaimed k-search jobs, running jobs,
                                    // records in the pool / block queues / spill ring, warps holding work

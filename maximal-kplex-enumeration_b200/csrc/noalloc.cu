@@ -149,7 +149,7 @@ extern "C" int kplex_search_noalloc(const uint32_t* d_off, const uint32_t* d_adj
         NA_CK(cudaStreamSynchronize(st));
         if (hc.error) {
             set_last_error(hc.error == KPLEX_ERR_NOMEM ? "root arena exceeds the 64 MiB no-allocation scratch"
-                                                       : "a root's subgraph exceeds 1024 vertices");
+                                                       : "a root's 2-hop subgraph exceeds 1024 vertices or its left set 8192");
             return out->status = (int)hc.error;
         }
         job_prefix_kernel<<<1, 1024, 0, st>>>(roots, nroots, job_base, &ctr->work);
