@@ -415,12 +415,23 @@ struct BnbSmem {
     uint16_t* gv;     // nmax
     uint16_t* pv;     // nmax
     unsigned long long* CT;   // 16 per-warp counters (lane 0 updates them; kept out of registers)
+    uint32_t* SCT;    // STACK_CACHE tags: the stack index each cached record was pushed at
+    uint32_t* SC;     // STACK_CACHE records of slot_words
     uint32_t* A;      // a_words: the current root's adjacency matrix, when it fits
 };
 
+// The newest STACK_CACHE records a warp pushes on its depth-first stack are
+// also kept in its shared memory (tagged with their stack index), so that the
+// usual pop, of the record pushed last, does not wait for an L2 round trip.
+constexpr uint32_t STACK_CACHE = 4;
+
+__host__ __device__ inline uint32_t stack_cache_words(uint32_t slot_words) {
+    return (STACK_CACHE * slot_words + STACK_CACHE + 3u) & ~3u;
+}
+
 __host__ __device__ inline uint32_t bnb_smem_words(uint32_t nmax, uint32_t slot_words, uint32_t a_words) {
     const uint32_t lists = 3 * ((nmax + 1) / 2);
-    return (((slot_words + 9 * MAX_WORDS + lists) + 3u) & ~3u) + 32u + a_words;
+    return (((slot_words + 9 * MAX_WORDS + lists) + 3u) & ~3u) + 32u + stack_cache_words(slot_words) + a_words;
 }
 
 __device__ inline BnbSmem bnb_smem(uint32_t* base, uint32_t nmax, uint32_t slot_words) {
@@ -440,7 +451,9 @@ __device__ inline BnbSmem bnb_smem(uint32_t* base, uint32_t nmax, uint32_t slot_
     m.gv = reinterpret_cast<uint16_t*>(p); p += (nmax + 1) / 2;
     m.pv = reinterpret_cast<uint16_t*>(p); p += (nmax + 1) / 2;
     m.CT = reinterpret_cast<unsigned long long*>(base + (((slot_words + 9 * MAX_WORDS + 3 * ((nmax + 1) / 2)) + 3u) & ~3u));
-    m.A = reinterpret_cast<uint32_t*>(m.CT + 16);
+    m.SCT = reinterpret_cast<uint32_t*>(m.CT + 16);
+    m.SC = m.SCT + STACK_CACHE;
+    m.A = m.SCT + stack_cache_words(slot_words);
     return m;
 }
 
@@ -659,8 +672,17 @@ __device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootVie
         uint32_t* dst = ww.stack + (ww.stop % sp.stack_depth) * SW;
         const uint32_t Cx = (l == vw) ? (Cw & ~vb) : Cw;
         const uint32_t Xx = (l == vw) ? (Xw | vb) : Xw;
-        if (l == 0) { __stcg(dst + 0, t->root); __stcg(dst + 1, np | ((nc - 1) << 16)); __stcg(dst + 2, nx + 1); __stcg(dst + 3, 0u); }
-        if (l < Wt) { __stcg(dst + 4 + l, Pw); __stcg(dst + 4 + Wt + l, Cx); __stcg(dst + 4 + 2 * Wt + l, Xx); }
+        uint32_t* cdst = m.SC + (uint32_t)(ww.stop % STACK_CACHE) * SW;   // shared-memory copy
+        if (l == 0) {
+            __stcg(dst + 0, t->root); __stcg(dst + 1, np | ((nc - 1) << 16)); __stcg(dst + 2, nx + 1); __stcg(dst + 3, 0u);
+            cdst[0] = t->root; cdst[1] = np | ((nc - 1) << 16); cdst[2] = nx + 1; cdst[3] = 0u;
+            m.SCT[ww.stop % STACK_CACHE] = (uint32_t)ww.stop;
+        }
+        if (l < Wt) {
+            __stcg(dst + 4 + l, Pw); __stcg(dst + 4 + Wt + l, Cx); __stcg(dst + 4 + 2 * Wt + l, Xx);
+            cdst[4 + l] = Pw; cdst[4 + Wt + l] = Cx; cdst[4 + 2 * Wt + l] = Xx;
+        }
+        __syncwarp();
         ++ww.stop;
         if (l == 0) { ++ww.tasks; ww.bb += 12ull * W; }
     }
@@ -851,6 +873,7 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
     uint32_t acc_graph = 0;
     unsigned long long* CT = m.CT;
     if (l < 16) CT[l] = 0ull;
+    if (l < STACK_CACHE) m.SCT[l] = 0xffffffffu;
     __syncwarp();
     WarpWork ww{sp.stacks + (uint64_t)warp * sp.stack_depth * SW, 0ull, 0ull,
                 CT[CT_CNT], CT[CT_HSUM], CT[CT_TASKS], CT[CT_NODES], CT[CT_BB]};
@@ -872,7 +895,9 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
         // ---------------- local depth-first work
         if (!have && ww.stop > ww.sbot) {
             --ww.stop;
-            load_record(ww.stack + (ww.stop % sp.stack_depth) * SW, Wt, &t, true);
+            const uint32_t cs = (uint32_t)(ww.stop % STACK_CACHE);
+            if (m.SCT[cs] == (uint32_t)ww.stop) load_record(m.SC + cs * SW, Wt, &t, false);   // still cached
+            else load_record(ww.stack + (ww.stop % sp.stack_depth) * SW, Wt, &t, true);
             have = true;
             __syncwarp();
         }
