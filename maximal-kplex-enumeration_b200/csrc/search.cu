@@ -974,8 +974,8 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
             }
             if (!paused) {
                 if (!ks_active) {
-                    // claim the next k-search job; ks_active rises before the claim so that
-                    // consumers never see "all jobs claimed" with a claim in flight
+                    // claim the next k-search job (its unit of work moves from "unclaimed"
+                    // to "running"); ks_active tells idle warps that k-search still runs
                     int j = -1;
                     if (l == 0 && *(volatile unsigned*)&sp.ctr->next_root < sp.njobs) {
                         atomicAdd(&sp.ctr->ks_active, 1u);
