@@ -37,3 +37,24 @@ def test_bad_params_rejected_before_device(kp):
         assert r["status"] == kp.ERR_PARAM, (k, q, r["status"])
     r = kp.enumerate_csr(off, adj, 2, 8, thres=0.0, check=False)
     assert r["status"] == kp.ERR_PARAM
+
+
+def test_no_silent_cpu_path_without_a_device(kp):
+    """Without a usable sm_100 device every device entry point fails with a status;
+    nothing falls back to a CPU computation."""
+    import pytest
+    if kp.device_ok():
+        pytest.skip("a CUDA device is present")
+    off, adj = kp.workload_graph("small")
+    r = kp.enumerate_csr(off, adj, 2, 8, check=False)
+    assert r["status"] == kp.ERR_NO_DEVICE and r["count"] == 0
+    graphs = kp.batch_workload(count=3, seed=4)
+    with pytest.raises(kp.KplexError) as e:
+        kp.enumerate_batch(graphs)
+    assert e.value.status == kp.ERR_NO_DEVICE
+    with pytest.raises(kp.KplexError) as e:
+        kp.autotune_batch(graphs, sample=2)
+    assert e.value.status == kp.ERR_NO_DEVICE
+    with pytest.raises(kp.KplexError) as e:
+        kp.Server(slots=1)
+    assert e.value.status == kp.ERR_NO_DEVICE
