@@ -139,29 +139,29 @@ def allreduce_results(dist, count: int, hsum: int, ms: float, device) -> tuple[i
     return int(tot[0].item()), int(tot[1].item()) & ((1 << 64) - 1), float(mx.item())
 
 
-def cpu_sample(off, adj, cfg, budget_s: float = 20.0):
-    """Oracle (OpenMP, all host cores) on a bounded root sample of the workload."""
+def cpu_sample(off, adj, cfg, budget_s: float = 20.0, span: int | None = None):
+    """Oracle (OpenMP, all host cores) on a bounded root sample of the workload: the
+    latest-ranked roots (where nearly all plexes of a degeneracy order lie), a range
+    grown 2x at a time from 1/1024 of the roots until one run takes budget_s / 4, or
+    exactly `span` roots when given.  Returns the baseline dict and the span used."""
     sys.path.insert(0, ROOT)
     import oracle  # CPU baseline only
 
     pre = oracle.preprocess(off, adj, cfg["k"], cfg["q"], cfg["truss"])
     nroots = max(0, pre["pn"] - cfg["q"] + 2)
-    # grow a contiguous range of the latest-ranked roots until the sample takes ~budget_s
-    span = max(1, nroots // 64)
-    best = None
+    fixed = span is not None
+    span = max(1, span if fixed else nroots // 1024)
     while True:
         b = max(0, nroots - span)
         t0 = time.perf_counter()
         r = oracle.enumerate_csr(off, adj, cfg["k"], cfg["q"], cfg["truss"], threads=0, root_begin=b, root_end=nroots)
         el = time.perf_counter() - t0
-        best = (r, el, b, nroots)
-        if el >= budget_s / 4 or span >= nroots:
+        if fixed or el >= budget_s / 4 or span >= nroots:
             break
-        span = min(nroots, span * 4)
-    r, el, b, e = best
+        span = min(nroots, span * 2)
     return {"value": r["count"] / el if el > 0 else 0.0, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
-            "sample": f"roots of degeneracy rank [{b},{e}) of {nroots}: {r['count']} plexes in {el:.2f} s "
-                      f"(oracle restatement, all {os.cpu_count()} host threads)"}
+            "sample": f"roots of degeneracy rank [{b},{nroots}) of {nroots}: {r['count']} plexes in {el:.2f} s "
+                      f"(oracle restatement, all {os.cpu_count()} host threads)"}, span
 
 
 def run_reference(args, cfg, off, adj):
@@ -169,8 +169,9 @@ def run_reference(args, cfg, off, adj):
     if rank != 0:
         return
     steps = []
+    span = None   # sized on the first (warm-up) step, then fixed
     for i in range(args.warmup + args.steps):
-        cb = cpu_sample(off, adj, cfg, budget_s=args.cpu_budget)
+        cb, span = cpu_sample(off, adj, cfg, budget_s=args.cpu_budget, span=span)
         if i >= args.warmup:
             steps.append(cb)
     v = statistics.median([s["value"] for s in steps])
@@ -492,7 +493,7 @@ def main():
         "clocks": clocks,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_sample(off, adj, cfg, budget_s=args.cpu_budget)
+        line["cpu_baseline"] = cpu_sample(off, adj, cfg, budget_s=args.cpu_budget)[0]
     if rank == 0:
         print(json.dumps(line), flush=True)
     prep.release()
