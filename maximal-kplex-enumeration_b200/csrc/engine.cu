@@ -397,11 +397,12 @@ int search_impl(kplex_prepared* h, Workspace* d, kplex_result* out, kplex_result
     cudaStream_t st = d->stream;
     const uint32_t nroots = h->nroots;
     uint32_t launches = 0;
-    cudaEvent_t e0, e1, ka, kb;
-    CK(cudaEventCreate(&e0));
-    CK(cudaEventCreate(&e1));
-    CK(cudaEventCreate(&ka));
-    CK(cudaEventCreate(&kb));
+    struct Events {   // destroyed on every return path
+        cudaEvent_t e[4] = {};
+        ~Events() { for (cudaEvent_t x : e) if (x) cudaEventDestroy(x); }
+    } evs;
+    for (cudaEvent_t& x : evs.e) CK(cudaEventCreate(&x));
+    cudaEvent_t e0 = evs.e[0], e1 = evs.e[1], ka = evs.e[2], kb = evs.e[3];
     CK(cudaEventRecord(e0, st));
     double ms_dec = 0, ms_bnb = 0;
     auto timed = [&](auto&& launch, double& acc) -> int {
@@ -553,10 +554,6 @@ int search_impl(kplex_prepared* h, Workspace* d, kplex_result* out, kplex_result
     CK(cudaEventSynchronize(e1));
     float ms = 0;
     CK(cudaEventElapsedTime(&ms, e0, e1));
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    cudaEventDestroy(ka);
-    cudaEventDestroy(kb);
     if (!hc.error && (hp.head != hp.tail || hc.work != 0)) { hc.error = KPLEX_ERR_TIMEOUT; g_last_error = "branch warps gave up with work left"; }
     if (per_graph) {
         const size_t G = h->ngraphs;
