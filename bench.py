@@ -360,7 +360,8 @@ def main():
     ap.add_argument("--duration", type=float, default=60.0, help="served: seconds of arrivals")
     ap.add_argument("--slots", type=int, default=2)
     ap.add_argument("--max-batch", type=int, default=256)
-    ap.add_argument("--split-grid", action="store_true")
+    ap.add_argument("--no-split-grid", dest="split_grid", action="store_false",
+                    help="served: give each launch the whole device instead of 1/slots of the SMs")
     ap.add_argument("--mem-budget", type=int, default=32, help="served: GiB")
     ap.add_argument("--shards", type=int, default=1,
                     help="plain, one GPU: search only the roots of rank r % shards == 0 (a small case for profiling)")

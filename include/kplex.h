@@ -212,6 +212,9 @@ typedef struct {
     float thres;             /* pause threshold, as kplex_params.thres (0 -> 0.25) */
     uint32_t flags;          /* KPLEX_FLAG_* applied to every launch */
     uint64_t pool_slots;     /* as kplex_params.pool_slots */
+    uint64_t large_bytes;    /* a request whose device estimate reaches this runs in a launch of its own,
+                                so small requests never wait inside a launch for a large one
+                                (0 -> 32 MiB, UINT64_MAX -> never) */
 } kplex_server_config;
 
 typedef struct {

@@ -5,8 +5,8 @@
 // Each of `slots` worker threads owns a Workspace (its own CUDA stream, arena,
 // task pool, branch stacks and spill ring).  A worker that is free admits, in
 // arrival order, every waiting request that fits the device-memory budget (up
-// to max_batch), preprocesses them on the host, uploads them and enumerates
-// them as one batched launch (prepare_set + search_impl, the path of
+// to max_batch; a request estimated at large_bytes or more goes alone),
+// preprocesses them on the host, uploads them and enumerates them as one batched launch (prepare_set + search_impl, the path of
 // kplex_enumerate_batch).  Requests that arrive meanwhile wait for the next free
 // worker, so while one launch searches, the next batch is preprocessed, uploaded
 // and decomposed on another stream.  With split_grid each launch's persistent
@@ -171,11 +171,14 @@ void kplex_server::worker(uint32_t slot) {
                     const uint64_t base = resident_locked();
                     while (!pending.empty() && batch.size() < max_batch) {
                         const uint64_t e = pending.front()->est_bytes;
+                        const bool large = e >= cfg.large_bytes;
+                        if (large && !batch.empty()) break;   // a large request gets a launch of its own
                         const bool alone = batch.empty() && inflight_bytes == 0;
                         if (!alone && base + add + e > cfg.mem_budget) break;   // arrival order: no overtaking
                         add += e;
                         batch.push_back(std::move(pending.front()));
                         pending.pop_front();
+                        if (large) break;
                     }
                     if (!batch.empty()) {
                         inflight_bytes += add;
@@ -212,6 +215,7 @@ int kplex_server_create(const kplex_server_config* cfg, kplex_server** out) {
     if (!s->cfg.max_batch) s->cfg.max_batch = 1024;
     if (!s->cfg.mem_budget) s->cfg.mem_budget = 16ull << 30;
     if (!(s->cfg.thres > 0.0f)) s->cfg.thres = 0.25f;
+    if (!s->cfg.large_bytes) s->cfg.large_bytes = 32ull << 20;
     s->device = cfg->device;
     for (uint32_t i = 0; i < s->cfg.slots; ++i) {
         s->ws.emplace_back(new Workspace());

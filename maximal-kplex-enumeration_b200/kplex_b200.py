@@ -71,7 +71,7 @@ class GenSpec(ctypes.Structure):
 class ServerConfig(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("slots", ctypes.c_uint32), ("max_batch", ctypes.c_uint32),
                 ("mem_budget", ctypes.c_uint64), ("split_grid", ctypes.c_uint32), ("thres", ctypes.c_float),
-                ("flags", ctypes.c_uint32), ("pool_slots", ctypes.c_uint64)]
+                ("flags", ctypes.c_uint32), ("pool_slots", ctypes.c_uint64), ("large_bytes", ctypes.c_uint64)]
 
 
 class Completion(ctypes.Structure):
@@ -413,8 +413,10 @@ class Server:
     and end-to-end latencies in ms."""
 
     def __init__(self, device: int = 0, slots: int = 2, max_batch: int = 1024, mem_budget: int = 16 << 30,
-                 split_grid: bool = False, thres: float = 0.25, flags: int = FLAG_QUIET, pool_slots: int = 0):
-        cfg = ServerConfig(device, slots, max_batch, mem_budget, 1 if split_grid else 0, thres, flags, pool_slots)
+                 split_grid: bool = False, thres: float = 0.25, flags: int = FLAG_QUIET, pool_slots: int = 0,
+                 large_bytes: int = 0):
+        cfg = ServerConfig(device, slots, max_batch, mem_budget, 1 if split_grid else 0, thres, flags, pool_slots,
+                           large_bytes)
         h = ctypes.c_void_p()
         rc = lib().kplex_server_create(ctypes.byref(cfg), ctypes.byref(h))
         if rc:
