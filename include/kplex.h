@@ -166,7 +166,9 @@ long long kplex_preprocess_csr(const uint32_t* offsets, const uint32_t* neighbor
  * Graphs whose scratch exceeds 64 MiB are rejected with KPLEX_ERR_NOMEM.  The
  * first call on a device looks up the array's device address (make it before
  * any stream capture); calls share the array, so calls that overlap on one
- * GPU race. */
+ * GPU race.  The inputs must be complete when the call starts (it runs on
+ * cudaStreamPerThread); p->device is made current during the call and the
+ * caller's device is restored.  ms_device is not measured (0). */
 int kplex_search_noalloc(const uint32_t* d_offsets, const uint32_t* d_neighbors, const int32_t* d_dpos,
                          const int32_t* d_dseq, const uint32_t* d_orig, uint32_t pn,
                          const kplex_params* p, kplex_result* out);

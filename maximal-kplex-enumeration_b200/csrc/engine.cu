@@ -198,6 +198,7 @@ int prepare_set(const std::vector<HostJob>& jobs, const kplex_params* p, Workspa
     kplex_prepared* h = new kplex_prepared();
     h->device = d->device;
     h->stream = d->stream;
+    if (cudaDeviceGetAttribute(&h->clock_khz, cudaDevAttrClockRate, d->device) != cudaSuccess) { cudaGetLastError(); h->clock_khz = 0; }
     h->p = *p;
     h->ngraphs = (uint32_t)G;
     h->ms_pre = ms_pre;
@@ -291,9 +292,12 @@ static void fill_result(const kplex_prepared* h, const Counters& hc, float ms, d
     out->roots_bytes = hc.roots_bytes;
     out->ks_tasks = hc.ks_tasks;
     out->stage_copies = hc.stage_copies;
-    out->ks_warp_ms = (double)hc.ks_cycles / (1.965e6);   // SM cycles at the 1965 MHz boost clock
-    out->bnb_warp_ms = (double)hc.bnb_cycles / (1.965e6);
-    out->idle_warp_ms = (double)hc.idle_cycles / (1.965e6);
+    // SM cycles converted at the device's rated clock; their ratios (the shares of warp
+    // time) do not depend on the clock the run actually saw
+    const double khz = h->clock_khz > 0 ? (double)h->clock_khz : 1.965e6;
+    out->ks_warp_ms = (double)hc.ks_cycles / khz;
+    out->bnb_warp_ms = (double)hc.bnb_cycles / khz;
+    out->idle_warp_ms = (double)hc.idle_cycles / khz;
     out->search_warps = search_warps;
     out->status = (int)hc.error;
 }
@@ -490,14 +494,11 @@ int search_impl(kplex_prepared* h, Workspace* d, kplex_result* out, kplex_result
     init_pool<<<d->sms * 4, 256, 0, st>>>(sp.pool_seq, cap, sp.pool);
     ++launches;
     const int warps_per_block = 8;
-    // tuning knobs (environment): blocks per SM the kernel is compiled for (2 or 3) and
-    // how many nodes a warp processes on one root before copying its A to shared memory
-    // (params first; the environment variables only fill in defaults)
-    const char* eb = getenv("KPLEX_BLOCKS_PER_SM");
-    int minb = P.blocks_per_sm ? (int)P.blocks_per_sm : (eb ? atoi(eb) : 2);
-    minb = minb == 3 ? 3 : 2;   // measured: 2 blocks x 128 registers beats 3 x 80 + spills
-    const char* es = getenv("KPLEX_STAGE_AFTER");
-    const int stage_after = P.stage_after ? P.stage_after : (es ? atoi(es) : 8);
+    // schedule knobs, from kplex_params only: blocks per SM the kernel is compiled for
+    // (2 or 3) and how many nodes a warp processes on one root before copying its A to
+    // shared memory
+    const int minb = P.blocks_per_sm == 3 ? 3 : 2;   // measured: 2 blocks x 128 registers beats 3 x 80 + spills
+    const int stage_after = P.stage_after ? P.stage_after : 8;
     sp.stage_after = stage_after > 0 ? (uint32_t)stage_after : 0u;
     auto kfn = minb == 2 ? search_kernel_2 : search_kernel_3;
     // stage adjacency matrices in shared memory when minb 8-warp blocks still fit on an SM

@@ -126,6 +126,7 @@ int device_state(int device, DeviceState** out);
 // root_base + nroots) of the concatenated root order.
 struct kplex_prepared {
     int device = 0;
+    int clock_khz = 0;               // the device's rated SM clock (cycle counters -> ms)
     cudaStream_t stream = nullptr;   // the workspace stream its buffers are ordered on
     kplex_params p{};
     uint32_t ngraphs = 0;

@@ -22,6 +22,12 @@
 // Every call reuses the same array, which keeps the previous call's
 // contents; everything that must start at zero is cleared on each call.
 // Two calls whose work overlaps on one GPU race on the array.
+//
+// The call works on cudaStreamPerThread, so the input buffers must be
+// complete before it starts (written on that stream or on the legacy default
+// stream, or synchronised); it returns after the search has finished.  It
+// makes p->device current while it runs and restores the caller's device.
+// ms_device is not measured (0); ms_total is the call's host wall time.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -65,6 +71,7 @@ using namespace kplex;
         cudaError_t e_ = (call);                                                    \
         if (e_ != cudaSuccess) {                                                    \
             set_last_error(std::string(#call) + ": " + cudaGetErrorString(e_));     \
+            if (out) out->status = KPLEX_ERR_CUDA;                                  \
             return KPLEX_ERR_CUDA;                                                  \
         }                                                                           \
     } while (0)
@@ -81,13 +88,21 @@ extern "C" int kplex_search_noalloc(const uint32_t* d_off, const uint32_t* d_adj
         return out->status = KPLEX_ERR_PARAM;
     }
     if (p->device < 0 || p->device >= 64) { set_last_error("bad device"); return out->status = KPLEX_ERR_PARAM; }
+    // the caller's current device is restored on every return after this point
+    int prev_device = -1;
+    if (cudaGetDevice(&prev_device) != cudaSuccess) { cudaGetLastError(); prev_device = -1; }
+    struct RestoreDevice {
+        int d;
+        ~RestoreDevice() { if (d >= 0) cudaSetDevice(d); }
+    } restore{prev_device};
+    auto finish = [&](int st) { out->status = st; return st; };
     NA_CK(cudaSetDevice(p->device));
     if (!g_na_ptr[p->device]) {   // set-up, once per device, with that device current
         void* ptr = nullptr;
         NA_CK(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
         cudaDeviceProp prop;
         NA_CK(cudaGetDeviceProperties(&prop, p->device));
-        if (prop.major != 10) { set_last_error("kernels are built for sm_100a only"); return out->status = KPLEX_ERR_NO_DEVICE; }
+        if (prop.major != 10) { set_last_error("kernels are built for sm_100a only"); return finish(KPLEX_ERR_NO_DEVICE); }
         g_na_sms[p->device] = prop.multiProcessorCount;
         g_na_ptr[p->device] = static_cast<uint32_t*>(ptr);
     }
@@ -112,7 +127,7 @@ extern "C" int kplex_search_noalloc(const uint32_t* d_off, const uint32_t* d_adj
     const size_t dec_bytes = (size_t)dec_warps * scratch_words * 4;
     if (off + dec_bytes + (1u << 20) > NOALLOC_BYTES) {
         set_last_error("graph too large for the 64 MiB no-allocation scratch (pn = " + std::to_string(pn) + ")");
-        return out->status = KPLEX_ERR_NOMEM;
+        return finish(KPLEX_ERR_NOMEM);
     }
     const size_t arena_off = off;
     const size_t dec_off = align_up(NOALLOC_BYTES - dec_bytes - 256, 256);
@@ -148,9 +163,10 @@ extern "C" int kplex_search_noalloc(const uint32_t* d_off, const uint32_t* d_adj
         NA_CK(cudaMemcpyAsync(&hc, ctr, sizeof(Counters), cudaMemcpyDeviceToHost, st));
         NA_CK(cudaStreamSynchronize(st));
         if (hc.error) {
-            set_last_error(hc.error == KPLEX_ERR_NOMEM ? "root arena exceeds the 64 MiB no-allocation scratch"
-                                                       : "a root's 2-hop subgraph exceeds 1024 vertices or its left set 8192");
-            return out->status = (int)hc.error;
+            set_last_error(hc.error == KPLEX_ERR_NOMEM      ? "root arena exceeds the 64 MiB no-allocation scratch"
+                           : hc.error == KPLEX_ERR_CAPACITY ? "a root's 2-hop subgraph exceeds 2048 vertices or its left set 8192"
+                                                            : "device error in decomposition");
+            return finish((int)hc.error);
         }
         job_prefix_kernel<<<1, 1024, 0, st>>>(roots, nroots, job_base, &ctr->work);
         ++launches;
@@ -181,7 +197,7 @@ extern "C" int kplex_search_noalloc(const uint32_t* d_off, const uint32_t* d_adj
     const size_t stacks_bytes = (size_t)blocks * warps_per_block * stack_per_warp;
     if (o2 + stacks_bytes + min_slots * rec_bytes + 512 > NOALLOC_BYTES) {
         set_last_error("task pool and stacks do not fit the 64 MiB no-allocation scratch");
-        return out->status = KPLEX_ERR_NOMEM;
+        return finish(KPLEX_ERR_NOMEM);
     }
     sp.stacks = reinterpret_cast<uint32_t*>(base + o2);
     o2 = align_up(o2 + stacks_bytes, 256);
@@ -206,7 +222,12 @@ extern "C" int kplex_search_noalloc(const uint32_t* d_off, const uint32_t* d_adj
     NA_CK(cudaMemcpyAsync(&hp, pool, sizeof(Pool), cudaMemcpyDeviceToHost, st));
     NA_CK(cudaStreamSynchronize(st));
     int status = (int)hc.error;
-    if (!status && nroots && hp.head != hp.tail) { status = KPLEX_ERR_TIMEOUT; set_last_error("records left in the pool"); }
+    // a bounded wait that gave up may leave work in k-search jobs, block queues or warp
+    // stacks while the pool itself is empty: the work counter covers all of them
+    if (!status && nroots && (hp.head != hp.tail || hc.work != 0 || hc.timeouts != 0)) {
+        status = KPLEX_ERR_TIMEOUT;
+        set_last_error("branch warps gave up with work left");
+    }
     out->count = hc.count;
     out->hash = hc.hash;
     out->valid_roots = hc.valid_roots;
@@ -220,7 +241,6 @@ extern "C" int kplex_search_noalloc(const uint32_t* d_off, const uint32_t* d_adj
     out->bnb_bytes = hc.bnb_bytes;
     out->roots_bytes = hc.roots_bytes;
     out->ms_total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-    out->ms_device = out->ms_total;
-    out->status = status;
-    return status;
+    out->ms_device = 0;   // not measured here (ms_total is the host wall time of the call)
+    return finish(status);
 }

@@ -74,9 +74,14 @@ struct Graph {
 enum : uint8_t { LP = 0, LC = 1, LX = 2, LU = 3, LH = 5 };                 // common.h:27-34
 enum : uint8_t { UNLINK2LESS = 0, LINK2LESS = 1, UNLINK2EQUAL = 2, LINK2EQUAL = 3, UNLINK2MORE = 4, LINK2MORE = 5 };  // common.h:37-44
 
-static const int MAX_BLK = 1024;   // common.h:8
-// Left sets may exceed MAX_BLK (the reference's buffers stop there); the
-// device build accepts up to 8192, so the oracle does too.
+// The reference keeps at most MAX_BLK_SIZE = 1024 one-hop neighbours of a root
+// (common.h:8): 1023 later ones and 1024 earlier ones in CSR order (src:87-131);
+// the rest are dropped.  That truncation is part of its semantics and is kept.
+static const int REF_BLK = 1024;
+// Capacity of a root's local subgraph (root, C1, C2).  The reference overruns
+// its 1024-entry buffers beyond REF_BLK (src:255); this restatement and the
+// device build accept up to 2048 local vertices and left sets up to 8192.
+static const int MAX_LOCAL = 2048;
 static const int MAX_LEFT = 8192;
 static const int MAX_DEPTH = 1000; // common.h:15
 
@@ -246,9 +251,9 @@ static bool decompose_root(const Graph& g, const std::vector<int>& dpos, const s
         uint32_t w = g.adj[j];
         if (pos < dpos[w]) later.push_back(w); else earlier.push_back(w);
     }
-    if (later.size() + 1 > (size_t)MAX_BLK || earlier.size() > (size_t)MAX_BLK) st.truncated++;
-    if (later.size() + 1 > (size_t)MAX_BLK) later.resize(MAX_BLK - 1);
-    if (earlier.size() > (size_t)MAX_BLK) earlier.resize(MAX_BLK);
+    if (later.size() + 1 > (size_t)REF_BLK || earlier.size() > (size_t)REF_BLK) st.truncated++;
+    if (later.size() + 1 > (size_t)REF_BLK) later.resize(REF_BLK - 1);
+    if (earlier.size() > (size_t)REF_BLK) earlier.resize(REF_BLK);
     // C1 peel, src:142-180: synchronous rounds until nothing is removed
     std::vector<uint32_t> c1 = later;
     for (;;) {
@@ -270,26 +275,32 @@ static bool decompose_root(const Graph& g, const std::vector<int>& dpos, const s
         for (uint32_t v : c1) if (in_sorted(g, u, v)) ++cnt;
         if (cnt >= lb2k + 1) left.push_back(u);
     }
-    // 2-hop scan, src:217-273 (visited = root, kept C1, kept left, scanned)
-    std::vector<uint32_t> vset; vset.push_back(r); vset.insert(vset.end(), c1.begin(), c1.end()); vset.insert(vset.end(), left.begin(), left.end());
-    std::sort(vset.begin(), vset.end());
-    std::vector<uint32_t> seen;  // scanned 2-hop candidates
+    // 2-hop scan, src:217-273 (visited = root, kept C1, kept left, scanned).
+    // Membership marks live in a per-thread array indexed by peeled id and are
+    // cleared before returning.
+    thread_local std::vector<uint8_t> mark;
+    if (mark.size() < g.n) mark.assign(g.n, 0);
+    std::vector<uint32_t> touched;
+    auto put = [&](uint32_t v) { if (!mark[v]) touched.push_back(v); mark[v] = 1; };
+    put(r);
+    for (uint32_t v : c1) put(v);
+    for (uint32_t v : left) put(v);
     std::vector<uint32_t> c2, left2;
     for (uint32_t nei : later) {
         for (uint32_t j = g.off[nei]; j < g.off[nei + 1]; ++j) {
             uint32_t w = g.adj[j];
-            if (std::binary_search(vset.begin(), vset.end(), w)) continue;
-            if (std::find(seen.begin(), seen.end(), w) != seen.end()) continue;
+            if (mark[w]) continue;   // visited, or already scanned
             const bool lat = pos < dpos[w];
             const int thr = lb2k + (lat ? 2 : 3);
             if (std::min<int>((int)g.deg[w], hop - 1) < thr) continue;
             int cnt = 0;
             for (uint32_t v : c1) if (in_sorted(g, w, v)) ++cnt;
-            seen.push_back(w);
+            put(w);
             if (lat) { if (cnt >= lb2k + 2) c2.push_back(w); }
             else { if (cnt >= lb2k + 3) left2.push_back(w); }
         }
     }
+    for (uint32_t v : touched) mark[v] = 0;
     std::sort(c2.begin(), c2.end());
     left.insert(left.end(), left2.begin(), left2.end());
     std::sort(left.begin(), left.end());
@@ -297,7 +308,7 @@ static bool decompose_root(const Graph& g, const std::vector<int>& dpos, const s
     s.n = n; s.nleft = (int)left.size();
     if (n < q) return false;
     st.valid++;
-    if (n > MAX_BLK || (int)left.size() > MAX_LEFT) { st.too_big++; return false; }
+    if (n > MAX_LOCAL || (int)left.size() > MAX_LEFT) { st.too_big++; return false; }
     {
         uint32_t cur = st.max_n.load(); while ((uint32_t)n > cur && !st.max_n.compare_exchange_weak(cur, n)) {}
         cur = st.max_left.load(); while ((uint32_t)left.size() > cur && !st.max_left.compare_exchange_weak(cur, (uint32_t)left.size())) {}
@@ -305,32 +316,47 @@ static bool decompose_root(const Graph& g, const std::vector<int>& dpos, const s
     s.n = n; s.hop = hop; s.nleft = (int)left.size(); s.root_rank = ri;
     s.gid.clear(); s.gid.push_back(r); s.gid.insert(s.gid.end(), c1.begin(), c1.end()); s.gid.insert(s.gid.end(), c2.begin(), c2.end());
     s.lgid = left;
-    // fillNeighbors src:405-443
+    // fillNeighbors src:405-443: local and left adjacency lists in ascending
+    // local (left) index, found through per-thread id -> index maps
+    thread_local std::vector<int32_t> lidx, leftidx;
+    if (lidx.size() < g.n) { lidx.assign(g.n, -1); leftidx.assign(g.n, -1); }
+    for (int i = 0; i < n; ++i) lidx[s.gid[i]] = i;
+    for (int j = 0; j < s.nleft; ++j) leftidx[left[j]] = j;
     s.nb.assign(n, {}); s.lnb.assign(n, {}); s.degHop.assign(n, 0);
     s.bits.assign(((size_t)n * n + 63) / 64, 0);
     s.cls.assign((size_t)n * n, 0);
     for (int i = 0; i < n; ++i) {
         const uint32_t o = s.gid[i];
-        int cnt = 0;
-        for (int j = 0; j < n; ++j) {
-            if (in_sorted(g, o, s.gid[j])) {
-                s.nb[i].push_back(j);
-                size_t c = (size_t)i * n + j; s.bits[c >> 6] |= 1ull << (c & 63);
-                s.cls[(size_t)i * n + j] = 1;
-                ++cnt;
-            }
-            if (j == hop - 1) s.degHop[i] = cnt;
+        for (uint32_t e = g.off[o]; e < g.off[o + 1]; ++e) {
+            const int j = lidx[g.adj[e]], jl = leftidx[g.adj[e]];
+            if (j >= 0) s.nb[i].push_back(j);
+            if (jl >= 0) s.lnb[i].push_back(jl);
         }
-        for (int j = 0; j < s.nleft; ++j) if (in_sorted(g, o, left[j])) s.lnb[i].push_back(j);
+        std::sort(s.nb[i].begin(), s.nb[i].end());
+        std::sort(s.lnb[i].begin(), s.lnb[i].end());
+        int cnt = 0;
+        for (int j : s.nb[i]) {
+            size_t c = (size_t)i * n + j; s.bits[c >> 6] |= 1ull << (c & 63);
+            s.cls[(size_t)i * n + j] = 1;
+            if (j < hop) ++cnt;
+        }
+        s.degHop[i] = cnt;
     }
+    for (int i = 0; i < n; ++i) lidx[s.gid[i]] = -1;
+    for (int j = 0; j < s.nleft; ++j) leftidx[left[j]] = -1;
     // buildCommonMtx src:1751-1853
     const int tPP1 = q - k - 2 * std::max(k - 2, 0), tPP2 = q - k - 2 * std::max(k - 3, 0);
     const int tPC1 = q - 2 * k - std::max(k - 2, 0), tPC2 = q - k - 1 - std::max(k - 2, 0) - std::max(k - 3, 0);
     const int tCC1 = q - 2 * k - (k - 1), tCC2 = q - 2 * k + 2 - (k - 1);
-    auto common = [&](int i, int j) {   // commonEle src:1727-1749
-        int a = 0, b = 0, c = 0;
-        const auto& A = s.nb[i]; const auto& B = s.nb[j];
-        while (a < s.degHop[i] && b < s.degHop[j]) { if (A[a] < B[b]) ++a; else if (A[a] > B[b]) ++b; else { ++c; ++a; ++b; } }
+    // commonEle src:1727-1749: common neighbours of i and j among local ids [0, hop),
+    // counted as the popcount of their adjacency rows restricted to [0, hop)
+    const int hw = (hop + 63) / 64;
+    std::vector<uint64_t> hb((size_t)n * hw, 0);
+    for (int i = 0; i < n; ++i)
+        for (int j : s.nb[i]) { if (j >= hop) break; hb[(size_t)i * hw + (j >> 6)] |= 1ull << (j & 63); }
+    auto common = [&](int i, int j) {
+        int c = 0;
+        for (int w = 0; w < hw; ++w) c += __builtin_popcountll(hb[(size_t)i * hw + w] & hb[(size_t)j * hw + w]);
         return c;
     };
     auto classify = [&](int i, int j, int t1, int t2) {
@@ -365,7 +391,7 @@ struct Ctx {
     std::vector<uint16_t> sat, commons;
     std::vector<uint32_t> uni;
     Ctx(const Sub& s_, const Params& p_, const std::vector<uint32_t>& o, Stats& st_) : s(s_), P(p_), orig(o), st(st_) {
-        sat.resize(MAX_BLK); commons.resize(MAX_LEFT); uni.assign(MAX_LEFT / 32, 0);
+        sat.resize(MAX_LOCAL); commons.resize(MAX_LEFT); uni.assign(MAX_LEFT / 32, 0);
     }
 };
 
