@@ -16,8 +16,8 @@
 // neighbours in C1 because q >= 2k-1 is required by the host).
 //
 // Per-warp scratch (global, L2 resident): loc[pn] maps a pruned id to its
-// local id (< 1024), to 1024 + left index, to EXCL, or NONE; cnt[pn] counts
-// C1 neighbours of 2-hop candidates.  Both are restored before the warp
+// local id (< MAX_LOCAL), to LOC_LEFT + left index, to EXCL, or NONE; cnt[pn]
+// counts C1 neighbours of 2-hop candidates.  Both are restored before the warp
 // moves to its next root.
 #include "warp.cuh"
 
@@ -25,19 +25,21 @@ namespace kplex {
 
 constexpr uint32_t LOC_NONE = 0xffffffffu;
 constexpr uint32_t LOC_EXCL = 0xfffffffeu;
+constexpr uint32_t LOC_LEFT = MAX_LOCAL;   // loc of left vertex i: LOC_LEFT + i
+constexpr int LATER_WORDS = REF_BLK / 32;  // bitset over the (at most 1023) later neighbours
 
 struct DecompScratch {
     uint32_t* loc;      // pn
     uint32_t* cnt;      // pn
-    uint32_t* later;    // MAX_LOCAL
-    uint32_t* earlier;  // MAX_LOCAL
+    uint32_t* later;    // REF_BLK
+    uint32_t* earlier;  // REF_BLK
     uint32_t* blk;      // MAX_LOCAL + 32 (root, C1, C2)
     uint32_t* left;     // MAX_LEFT + 32
     uint32_t* tmp;      // MAX_LEFT + 32
 };
 
 __host__ __device__ inline uint64_t decomp_scratch_words(uint32_t pn) {
-    return 2ull * pn + 2 * MAX_LOCAL + (MAX_LOCAL + 32) + 2 * (MAX_LEFT + 32) + 64;
+    return 2ull * pn + 2 * REF_BLK + (MAX_LOCAL + 32) + 2 * (MAX_LEFT + 32) + 64;
 }
 
 __device__ inline DecompScratch decomp_scratch(const SearchParams& sp, unsigned warp) {
@@ -45,8 +47,8 @@ __device__ inline DecompScratch decomp_scratch(const SearchParams& sp, unsigned 
     DecompScratch s;
     s.loc = b; b += sp.pn;
     s.cnt = b; b += sp.pn;
-    s.later = b; b += MAX_LOCAL;
-    s.earlier = b; b += MAX_LOCAL;
+    s.later = b; b += REF_BLK;
+    s.earlier = b; b += REF_BLK;
     s.blk = b; b += MAX_LOCAL + 32;
     s.left = b; b += MAX_LEFT + 32;
     s.tmp = b;
@@ -81,7 +83,7 @@ __global__ void __launch_bounds__(256) decompose_kernel(SearchParams sp) {
     const unsigned l = lane_id();
     const unsigned warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     DecompScratch S = decomp_scratch(sp, warp);
-    __shared__ uint32_t s_alive_all[8][MAX_WORDS];
+    __shared__ uint32_t s_alive_all[8][LATER_WORDS];
     __shared__ uint32_t s_row_all[8][MAX_WORDS + MAX_LEFT_WORDS];
     uint32_t* s_alive = s_alive_all[threadIdx.x >> 5];
     uint32_t* s_row = s_row_all[threadIdx.x >> 5];
@@ -131,17 +133,17 @@ __global__ void __launch_bounds__(256) decompose_kernel(SearchParams sp) {
             const unsigned below = (1u << l) - 1;
             if (valid && lat) {
                 const int idx = nlater + __popc(ml & below);
-                if (idx < MAX_LOCAL - 1) S.later[idx] = w;
+                if (idx < REF_BLK - 1) S.later[idx] = w;
             }
             if (valid && !lat) {
                 const int idx = nearlier + __popc(me & below);
-                if (idx < MAX_LOCAL) S.earlier[idx] = w;
+                if (idx < REF_BLK) S.earlier[idx] = w;
             }
             nlater += __popc(ml);
             nearlier += __popc(me);
         }
-        if (nlater > MAX_LOCAL - 1) { nlater = MAX_LOCAL - 1; truncated = true; }
-        if (nearlier > MAX_LOCAL) { nearlier = MAX_LOCAL; truncated = true; }
+        if (nlater > REF_BLK - 1) { nlater = REF_BLK - 1; truncated = true; }
+        if (nearlier > REF_BLK) { nearlier = REF_BLK; truncated = true; }
         __syncwarp();
         // loc: later j -> j (temporary), earlier -> EXCL until the left filter
         for (int i = l; i < nlater; i += 32) loc[S.later[i]] = (uint32_t)i;
@@ -180,11 +182,11 @@ __global__ void __launch_bounds__(256) decompose_kernel(SearchParams sp) {
             }
             __syncwarp();
             if (removed == 0) break;
-            if (l < MAX_WORDS) { s_alive[l] &= ~s_row[MAX_WORDS + l]; s_row[MAX_WORDS + l] = 0; }
+            if (l < LATER_WORDS) { s_alive[l] &= ~s_row[MAX_WORDS + l]; s_row[MAX_WORDS + l] = 0; }
             __syncwarp();
             alive -= removed;
         }
-        if (l < MAX_WORDS) s_row[MAX_WORDS + l] = 0;
+        if (l < LATER_WORDS) s_row[MAX_WORDS + l] = 0;
         __syncwarp();
 
         int hop = 0, n = 0, nleft = 0;
@@ -217,7 +219,7 @@ __global__ void __launch_bounds__(256) decompose_kernel(SearchParams sp) {
                 if (c >= lb2k + 1) { if (l == 0) S.left[nl1] = u; ++nl1; }
             }
             __syncwarp();
-            for (int i = l; i < nl1; i += 32) loc[S.left[i]] = 1024u + (uint32_t)i;  // marks membership
+            for (int i = l; i < nl1; i += 32) loc[S.left[i]] = LOC_LEFT + (uint32_t)i;  // marks membership
             __syncwarp();
 
             // ---- 2-hop scan (src:217-273): count C1 neighbours of unvisited vertices
@@ -269,9 +271,9 @@ __global__ void __launch_bounds__(256) decompose_kernel(SearchParams sp) {
 
         const bool valid = !skip && n >= q;
         if (valid && !oversized) {
-            // final loc: blk -> local id, left -> 1024 + index
+            // final loc: blk -> local id, left -> LOC_LEFT + index
             for (int i = l; i < n; i += 32) loc[S.blk[i]] = (uint32_t)i;
-            for (int i = l; i < nleft; i += 32) loc[S.left[i]] = 1024u + (uint32_t)i;
+            for (int i = l; i < nleft; i += 32) loc[S.left[i]] = LOC_LEFT + (uint32_t)i;
             __syncwarp();
             const uint32_t W = ((uint32_t)((n + 31) >> 5) + 3u) & ~3u;
             const uint32_t WL = nleft ? ((uint32_t)((nleft + 31) >> 5) + 3u) & ~3u : 0u;
@@ -300,14 +302,14 @@ __global__ void __launch_bounds__(256) decompose_kernel(SearchParams sp) {
                     for (uint32_t j = sp.off[u] + l; j < sp.off[u + 1]; j += 32) {
                         const uint32_t x = loc[sp.adj[j]];
                         if (x < (uint32_t)n) atomicOr(&s_row[x >> 5], 1u << (x & 31));
-                        else if (x >= 1024u && x < 1024u + (uint32_t)nleft) {
-                            const uint32_t jl = x - 1024u;
+                        else if (x >= LOC_LEFT && x < LOC_LEFT + (uint32_t)nleft) {
+                            const uint32_t jl = x - LOC_LEFT;
                             atomicOr(&s_row[MAX_WORDS + (jl >> 5)], 1u << (jl & 31));
                             atomicOr(&LT[(uint64_t)jl * W + (i >> 5)], 1u << (i & 31));
                         }
                     }
                     __syncwarp();
-                    if (l < W) A[(uint64_t)i * W + l] = s_row[l];
+                    for (uint32_t w = l; w < W; w += 32) A[(uint64_t)i * W + w] = s_row[w];
                     for (uint32_t w = l; w < WL; w += 32) LA[(uint64_t)i * WL + w] = s_row[MAX_WORDS + w];
                     __syncwarp();
                 }

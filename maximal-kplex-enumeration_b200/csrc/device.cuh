@@ -23,7 +23,14 @@
 
 namespace kplex {
 
-constexpr int MAX_LOCAL = 1024;     // inc/common.h:8 MAX_BLK_SIZE
+// The reference keeps at most MAX_BLK_SIZE = 1024 one-hop neighbours of a root
+// (inc/common.h:8): 1023 later and 1024 earlier ones in CSR order, dropping the
+// rest (src:87-131).  That truncation is part of its results and is kept.
+constexpr int REF_BLK = 1024;
+// A root's local subgraph (root, C1, C2) may hold up to MAX_LOCAL vertices.  The
+// reference overruns its 1024-entry buffers beyond REF_BLK (src:255); here a
+// warp keeps one bitset word per lane up to 1024 vertices and two beyond.
+constexpr int MAX_LOCAL = 2048;
 constexpr int MAX_WORDS = MAX_LOCAL / 32;
 // The left set (earlier-ordered vertices that may extend an output) is only
 // read by the maximality check, so it may be larger than the local subgraph;
@@ -31,14 +38,19 @@ constexpr int MAX_WORDS = MAX_LOCAL / 32;
 // (src:117-121, 262, 706-841).
 constexpr int MAX_LEFT = 8192;
 constexpr int MAX_LEFT_WORDS = MAX_LEFT / 32;
-constexpr int KS_MAX_DEPTH = 1000;  // inc/common.h:15 MAX_DEPTH
+// The reference's k-search stack holds 1000 frames (inc/common.h:15 MAX_DEPTH) and
+// abandons the rest of a root when it would go deeper (src:1987-1991), losing
+// results on roots with about 1000 or more C2 vertices.  A path pushes at most
+// one frame per C2 vertex plus a leaf frame, so n + 8 frames (n = the root's
+// local vertices) never fill and no root is abandoned here.
+constexpr int KS_MAX_DEPTH = MAX_LOCAL + 8;
 constexpr int MAX_K = 32;
 
 // root flags
 enum : uint32_t {
     ROOT_VALID = 1u,       // |blk| >= q: counted in "Total Valid Blocks"
     ROOT_TRUNCATED = 2u,   // more than 1023 later or 1024 earlier neighbours (reference drops extras)
-    ROOT_OVERSIZED = 4u,   // n or |left| beyond 1024: not representable, run fails
+    ROOT_OVERSIZED = 4u,   // n beyond MAX_LOCAL or |left| beyond MAX_LEFT: the run fails
     ROOT_SKIPPED = 8u,     // C1 smaller than q-k after peeling (src:148)
 };
 
@@ -152,6 +164,14 @@ struct SearchParams {
     uint32_t njobs;
     unsigned long long spin_limit;   // iterations for any bounded wait
 };
+
+// The persistent search kernel, one instantiation per bitset width (words per
+// lane, 1 or 2) and blocks per SM (2 or 3): search.cu.
+using SearchKernel = void (*)(SearchParams, uint32_t);
+SearchKernel search_kernel_for(uint32_t words_per_lane, int blocks_per_sm);
+uint32_t search_words_per_lane(uint32_t max_w);   // 2 when a root's rows exceed 32 words
+uint32_t bnb_smem_words_host(uint32_t nmax, uint32_t slot_words, uint32_t a_words, uint32_t words_per_lane);
+uint32_t ks_slot_words_host(uint32_t nmax, uint32_t slot_words, uint32_t words_per_lane);
 
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31; }
 

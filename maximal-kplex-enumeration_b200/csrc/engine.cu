@@ -29,12 +29,8 @@
 namespace kplex {
 
 __global__ void decompose_kernel(SearchParams sp);
-__global__ void search_kernel_3(SearchParams sp, uint32_t nmax);
-__global__ void search_kernel_2(SearchParams sp, uint32_t nmax);
 __global__ void job_prefix_kernel(const RootDesc* roots, uint32_t nroots, uint32_t* job_base, unsigned int* work);
 uint64_t decomp_scratch_words_host(uint32_t pn);
-uint32_t bnb_smem_words_host(uint32_t nmax, uint32_t slot_words, uint32_t a_words);
-uint32_t ks_slot_words_host(uint32_t nmax, uint32_t slot_words);
 
 // ------------------------------------------------------------------ small kernels
 __global__ void init_decomp_scratch(uint32_t* scratch, uint64_t words_per_warp, uint32_t pn, uint32_t nwarps) {
@@ -55,9 +51,6 @@ __global__ void init_ks_slots(uint32_t* slots, uint32_t nwarps, uint32_t words) 
 
 // ------------------------------------------------------------------ errors
 static thread_local std::string g_last_error;
-
-__global__ void search_kernel_2(SearchParams sp, uint32_t nmax);
-__global__ void search_kernel_3(SearchParams sp, uint32_t nmax);
 
 int workspace_init(Workspace& w, int device, int sms) {
     w.device = device;
@@ -85,8 +78,9 @@ int device_state(int device, DeviceState** out) {
         d.sms = prop.multiProcessorCount;
         // the dynamic shared-memory cap is raised once to the per-block maximum, so
         // that concurrent searches never race on a per-function attribute
-        CK(cudaFuncSetAttribute(search_kernel_2, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
-        CK(cudaFuncSetAttribute(search_kernel_3, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+        for (uint32_t nw : {1u, 2u})
+            for (int minb : {2, 3})
+                CK(cudaFuncSetAttribute(search_kernel_for(nw, minb), cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
         int rc = workspace_init(d.ws, device, d.sms);
         if (rc) return rc;
         d.init = true;
@@ -121,7 +115,7 @@ struct Replay {
     SearchParams sp{};
     uint32_t dec_warps = 0, blocks = 0, nmax = 0, launches = 0;
     size_t smem = 0;
-    bool minb3 = false;
+    SearchKernel kfn = nullptr;
     unsigned long long cap = 0, scap = 0;
     cudaGraphExec_t exec = nullptr;
     bool exec_per_graph = false;
@@ -313,7 +307,7 @@ static int replay_capture(kplex_prepared* h, Replay& r, Workspace* d, bool per_g
         CK(cudaMallocHost(&r.h_gh, G * 8));
         CK(cudaMallocHost(&r.h_gv, G * 4));
     }
-    auto kfn = r.minb3 ? search_kernel_3 : search_kernel_2;
+    const SearchKernel kfn = r.kfn;
     // events become event-record nodes of the graph (external records), so that the
     // host can wait on the last one and time the phases after a replay
     CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
@@ -465,7 +459,7 @@ int search_impl(kplex_prepared* h, Workspace* d, kplex_result* out, kplex_result
         break;
     }
     if (hc.error) {
-        g_last_error = hc.error == KPLEX_ERR_CAPACITY ? "a root's 2-hop subgraph exceeds 1024 vertices or its left set 8192"
+        g_last_error = hc.error == KPLEX_ERR_CAPACITY ? "a root's 2-hop subgraph exceeds 2048 vertices or its left set 8192"
                                                       : "device error in decomposition";
         return (int)hc.error;
     }
@@ -500,13 +494,16 @@ int search_impl(kplex_prepared* h, Workspace* d, kplex_result* out, kplex_result
     const int minb = P.blocks_per_sm == 3 ? 3 : 2;   // measured: 2 blocks x 128 registers beats 3 x 80 + spills
     const int stage_after = P.stage_after ? P.stage_after : 8;
     sp.stage_after = stage_after > 0 ? (uint32_t)stage_after : 0u;
-    auto kfn = minb == 2 ? search_kernel_2 : search_kernel_3;
+    // one bitset word per lane while every root fits 1024 vertices, two beyond
+    const uint32_t nw = search_words_per_lane(hc.max_w);
+    const SearchKernel kfn = search_kernel_for(nw, minb);
     // stage adjacency matrices in shared memory when minb 8-warp blocks still fit on an SM
     int per_sm = 0;
     size_t smem_bytes = 0;
     for (int stage = sp.stage_after ? 1 : 0; stage >= 0; --stage) {
         sp.a_words = stage ? ((hc.max_nw + 3u) & ~3u) : 0u;
-        smem_bytes = (size_t)(ks_slot_words_host(nmax, sp.slot_words) + warps_per_block * bnb_smem_words_host(nmax, sp.slot_words, sp.a_words)) * 4;
+        smem_bytes = (size_t)(ks_slot_words_host(nmax, sp.slot_words, nw) +
+                              warps_per_block * bnb_smem_words_host(nmax, sp.slot_words, sp.a_words, nw)) * 4;
         if (smem_bytes > 227 * 1024) continue;
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, warps_per_block * 32, smem_bytes));
         if (per_sm >= minb || !stage) break;
@@ -584,7 +581,7 @@ int search_impl(kplex_prepared* h, Workspace* d, kplex_result* out, kplex_result
         r->blocks = blocks;
         r->nmax = nmax;
         r->smem = smem_bytes;
-        r->minb3 = (minb == 3);
+        r->kfn = kfn;
         r->cap = cap;
         r->scap = sp.spill_on ? scap_used : 0;
         r->launches = launches;
@@ -635,7 +632,7 @@ const char* kplex_status_string(int s) {
         case KPLEX_ERR_FORMAT: return "malformed graph";
         case KPLEX_ERR_CUDA: return "cuda error";
         case KPLEX_ERR_NOMEM: return "out of memory";
-        case KPLEX_ERR_CAPACITY: return "root subgraph exceeds 1024 vertices (or its left set 8192)";
+        case KPLEX_ERR_CAPACITY: return "root subgraph exceeds 2048 vertices (or its left set 8192)";
         case KPLEX_ERR_TIMEOUT: return "bounded device wait gave up";
         case KPLEX_ERR_NO_DEVICE: return "no usable CUDA device";
         case KPLEX_ERR_INTERNAL: return "internal device check failed";

@@ -45,13 +45,10 @@ constexpr size_t NOALLOC_BYTES = 64ull << 20;
 static __device__ __align__(256) uint32_t g_noalloc_scratch[NOALLOC_BYTES / 4];
 
 __global__ void decompose_kernel(SearchParams sp);
-__global__ void search_kernel_3(SearchParams sp, uint32_t nmax);
 __global__ void init_decomp_scratch(uint32_t* scratch, uint64_t words_per_warp, uint32_t pn, uint32_t nwarps);
 __global__ void init_pool(uint32_t* seq, unsigned long long cap, Pool* pool);
 __global__ void job_prefix_kernel(const RootDesc* roots, uint32_t nroots, uint32_t* job_base, unsigned int* work);
 uint64_t decomp_scratch_words_host(uint32_t pn);
-uint32_t bnb_smem_words_host(uint32_t nmax, uint32_t slot_words, uint32_t a_words);
-uint32_t ks_slot_words_host(uint32_t nmax, uint32_t slot_words);
 void set_last_error(const std::string& msg);
 
 namespace {
@@ -184,10 +181,13 @@ extern "C" int kplex_search_noalloc(const uint32_t* d_off, const uint32_t* d_adj
     size_t o2 = align_up(arena_off + (size_t)hc.arena_top * 4, 256);
     const int warps_per_block = 8;
     sp.a_words = 0;
-    const size_t smem_bytes = (size_t)(ks_slot_words_host(nmax, sp.slot_words) + warps_per_block * bnb_smem_words_host(nmax, sp.slot_words, 0)) * 4;
-    NA_CK(cudaFuncSetAttribute(search_kernel_3, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+    const uint32_t nw = search_words_per_lane(Wt);
+    const SearchKernel kfn = search_kernel_for(nw, 3);
+    const size_t smem_bytes = (size_t)(ks_slot_words_host(nmax, sp.slot_words, nw) +
+                                       warps_per_block * bnb_smem_words_host(nmax, sp.slot_words, 0, nw)) * 4;
+    NA_CK(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
     int per_sm = 0;
-    NA_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, search_kernel_3, warps_per_block * 32, smem_bytes));
+    NA_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, warps_per_block * 32, smem_bytes));
     uint32_t blocks = (uint32_t)sms * (uint32_t)std::max(per_sm, 1);
     sp.stack_depth = nmax + 2;
     const size_t stack_per_warp = (size_t)sp.stack_depth * sp.slot_words * 4;
@@ -213,7 +213,7 @@ extern "C" int kplex_search_noalloc(const uint32_t* d_off, const uint32_t* d_adj
     init_pool<<<sms * 4, 256, 0, st>>>(sp.pool_seq, cap, sp.pool);
     ++launches;
     if (nroots) {
-        search_kernel_3<<<blocks, warps_per_block * 32, smem_bytes, st>>>(sp, nmax);
+        kfn<<<blocks, warps_per_block * 32, smem_bytes, st>>>(sp, nmax);
         ++launches;
         NA_CK(cudaGetLastError());
     }

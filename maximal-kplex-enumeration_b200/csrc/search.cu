@@ -21,6 +21,11 @@
 //    reference gets from its queues B and C).
 // neiInG / neiInP, which the reference stores per task (u16 arrays, common.h:144-170),
 // are recomputed from the bitsets: neiInG[v] = |N(v) ∩ (P ∪ C)|, neiInP[v] = |N(v) ∩ P|.
+//
+// A bitset over a root's local vertices is held by the warp in registers, NW
+// words per lane: lane l holds words l, l + 32, ... (NW = 1 covers 1024
+// vertices, NW = 2 covers MAX_LOCAL = 2048).  The kernel is compiled for both;
+// a search uses NW = 2 only when one of its roots has more than 1024 vertices.
 #include "warp.cuh"
 #include <climits>
 
@@ -55,26 +60,112 @@ __device__ __forceinline__ RootView root_view(const SearchParams& sp, uint32_t r
     return v;
 }
 
+// ============================================================== per-lane bitset words
+// Bits<NW>: this lane's NW words of a bitset of 32 * NW words (word l + 32 j in
+// w[j]).  Every index into w[] is a compile-time constant after unrolling, so
+// the words stay in registers.
+template <int NW>
+struct Bits {
+    uint32_t w[NW];
+};
+
+template <int NW>
+__device__ __forceinline__ Bits<NW> bits_zero() {
+    Bits<NW> b;
+#pragma unroll
+    for (int j = 0; j < NW; ++j) b.w[j] = 0u;
+    return b;
+}
+// words l + 32 j of p, 0 at and beyond word `nwords`
+template <int NW>
+__device__ __forceinline__ Bits<NW> bits_load(const uint32_t* p, uint32_t nwords) {
+    Bits<NW> b;
+    const unsigned l = lane_id();
+#pragma unroll
+    for (int j = 0; j < NW; ++j) b.w[j] = (l + 32u * j < nwords) ? p[l + 32u * j] : 0u;
+    return b;
+}
+template <int NW>
+__device__ __forceinline__ Bits<NW> bits_ldg(const uint32_t* p, uint32_t nwords) {
+    Bits<NW> b;
+    const unsigned l = lane_id();
+#pragma unroll
+    for (int j = 0; j < NW; ++j) b.w[j] = (l + 32u * j < nwords) ? __ldg(p + l + 32u * j) : 0u;
+    return b;
+}
+// all 32 * NW words to a shared-memory array
+template <int NW>
+__device__ __forceinline__ void bits_store(uint32_t* p, const Bits<NW>& b) {
+    const unsigned l = lane_id();
+#pragma unroll
+    for (int j = 0; j < NW; ++j) p[l + 32u * j] = b.w[j];
+}
+template <int NW>
+__device__ __forceinline__ void bits_fill(uint32_t* p, uint32_t v) {
+    const unsigned l = lane_id();
+#pragma unroll
+    for (int j = 0; j < NW; ++j) p[l + 32u * j] = v;
+}
+template <int NW>
+__device__ __forceinline__ int bits_count(const Bits<NW>& b) {
+    int c = 0;
+#pragma unroll
+    for (int j = 0; j < NW; ++j) c += __popc(b.w[j]);
+    return warp_sum(c);
+}
+// OR `m` into word `wi` (held by lane wi % 32, slot wi / 32)
+template <int NW>
+__device__ __forceinline__ void bits_or_word(Bits<NW>& b, uint32_t wi, uint32_t m) {
+    if ((wi & 31u) != lane_id()) return;
+#pragma unroll
+    for (int j = 0; j < NW; ++j) if ((wi >> 5) == (uint32_t)j) b.w[j] |= m;
+}
+template <int NW>
+__device__ __forceinline__ void bits_set(Bits<NW>& b, uint32_t v) { bits_or_word(b, v >> 5, 1u << (v & 31)); }
+template <int NW>
+__device__ __forceinline__ void bits_clear(Bits<NW>& b, uint32_t v) {
+    if (((v >> 5) & 31u) != lane_id()) return;
+#pragma unroll
+    for (int j = 0; j < NW; ++j) if ((v >> 10) == (uint32_t)j) b.w[j] &= ~(1u << (v & 31));
+}
+template <int NW>
+__device__ __forceinline__ Bits<NW> bits_or(const Bits<NW>& a, const Bits<NW>& b) {
+    Bits<NW> r;
+#pragma unroll
+    for (int j = 0; j < NW; ++j) r.w[j] = a.w[j] | b.w[j];
+    return r;
+}
+// ascending list of the set bits' indices; returns their count
+template <int NW>
+__device__ __forceinline__ int bits_list(const Bits<NW>& b, uint16_t* list) {
+    int off = 0;
+#pragma unroll
+    for (int j = 0; j < NW; ++j) off += bits_to_list(b.w[j], list + off, 1024u * j);
+    return off;
+}
+
 // ============================================================== k-search state (shared memory)
 // Layout in words, sized by the largest root n_max of the search:
 //   hdr (root, sz, np, nc2) | P stack [MAX_K] | frames | C2 list | C1 tags | C2 tags |
-//   C1 member list | C1, X, P bitsets [3 x 32] | scratch masks [3 x 32]
-// Along any stack path every pushed frame moves one C2 vertex to X or P (the
-// last push may add one leaf frame), so min(n_max + 8, KS_MAX_DEPTH + 8) frames suffice.
-struct KsLayout { uint32_t fr, c2, t1, t2, lst, bits, aux, total; };
+//   C1 member list | C1, X, P bitsets [3 x BW] | scratch masks [3 x BW]
+// with BW = 32 * NW.  Along any stack path every pushed frame moves one C2
+// vertex to X or P (the last push may add one leaf frame), so n_max + 8
+// frames suffice.
+struct KsLayout { uint32_t fr, c2, t1, t2, lst, bits, aux, total, bw; };
 
-__host__ __device__ inline KsLayout ks_layout(uint32_t nmax) {
+__host__ __device__ inline KsLayout ks_layout(uint32_t nmax, uint32_t nw) {
     KsLayout L;
+    L.bw = 32 * nw;
     uint32_t o = 8 + MAX_K;
-    const uint32_t frames = ((nmax + 8 < (uint32_t)KS_MAX_DEPTH + 8 ? nmax + 8 : (uint32_t)KS_MAX_DEPTH + 8) + 3u) & ~3u;
+    const uint32_t frames = ((nmax + 8 < (uint32_t)KS_MAX_DEPTH ? nmax + 8 : (uint32_t)KS_MAX_DEPTH) + 3u) & ~3u;
     const uint32_t half = (((nmax + 1) / 2) + 3u) & ~3u;
     L.fr = o; o += frames;
     L.c2 = o; o += half;
     L.t1 = o; o += half;
     L.t2 = o; o += half;
     L.lst = o; o += half;
-    L.bits = o; o += 3 * MAX_WORDS;
-    L.aux = o; o += 3 * MAX_WORDS;
+    L.bits = o; o += 3 * L.bw;
+    L.aux = o; o += 3 * L.bw;
     L.total = o;
     return L;
 }
@@ -88,7 +179,9 @@ __device__ __forceinline__ uint32_t fr_br(uint32_t f) { return (f >> 8) & 0xff; 
 __device__ __forceinline__ uint32_t fr_st(uint32_t f) { return (f >> 16) & 0xf; }
 __device__ __forceinline__ uint32_t fr_v(uint32_t f) { return f >> 20; }
 
+template <int NW>
 struct KsSlot {
+    static constexpr uint32_t BW = 32 * NW;
     uint32_t* w;
     KsLayout L;
     __device__ uint32_t& root() const { return w[0]; }
@@ -101,10 +194,12 @@ struct KsSlot {
     __device__ uint16_t* t1() const { return reinterpret_cast<uint16_t*>(w + L.t1); }
     __device__ uint16_t* t2() const { return reinterpret_cast<uint16_t*>(w + L.t2); }
     __device__ uint16_t* lst() const { return reinterpret_cast<uint16_t*>(w + L.lst); }
-    __device__ uint32_t* bits() const { return w + L.bits; }
+    __device__ uint32_t* c1bits() const { return w + L.bits; }
+    __device__ uint32_t* xbits() const { return w + L.bits + BW; }
+    __device__ uint32_t* pbits() const { return w + L.bits + 2 * BW; }
     __device__ uint32_t* mask() const { return w + L.aux; }
-    __device__ uint32_t* aux() const { return w + L.aux + MAX_WORDS; }
-    __device__ uint32_t* keep() const { return w + L.aux + 2 * MAX_WORDS; }
+    __device__ uint32_t* aux() const { return w + L.aux + BW; }
+    __device__ uint32_t* keep() const { return w + L.aux + 2 * BW; }
 };
 
 // Initial state of k-search job (r, d).  The reference's k-search for a root
@@ -118,20 +213,24 @@ struct KsSlot {
 // that frame from state 2 on; job m is the chain's bottom (C2 empty, state 0).
 // The jobs are independent, so one root's k-search spreads over many warps,
 // and their emissions are the reference's emissions for the root.
-__device__ void ks_start(const SearchParams& sp, const KsSlot& S, uint32_t r, uint32_t d, const RootDesc& rd) {
+template <int NW>
+__device__ void ks_start(const SearchParams& sp, const KsSlot<NW>& S, uint32_t r, uint32_t d, const RootDesc& rd) {
     const unsigned l = lane_id();
     const uint32_t n = rd.n, hop = rd.hop, m = n - hop;
     const uint32_t keep = m - d;   // C2 list = [hop, hop + keep), X = [hop + keep, n)
-    const uint32_t lo = l * 32;
-    uint32_t c1 = 0, x = 0;
-    for (uint32_t b = 0; b < 32; ++b) {
-        const uint32_t v = lo + b;
-        if (v >= 1 && v < hop) c1 |= 1u << b;
-        if (v >= hop + keep && v < n) x |= 1u << b;
+#pragma unroll
+    for (int j = 0; j < NW; ++j) {
+        const uint32_t wi = l + 32u * j, lo = wi * 32;
+        uint32_t c1 = 0, x = 0;
+        for (uint32_t b = 0; b < 32; ++b) {
+            const uint32_t v = lo + b;
+            if (v >= 1 && v < hop) c1 |= 1u << b;
+            if (v >= hop + keep && v < n) x |= 1u << b;
+        }
+        S.c1bits()[wi] = c1;
+        S.xbits()[wi] = x;
+        S.pbits()[wi] = (wi == 0) ? 1u : 0u;
     }
-    S.bits()[l] = c1;
-    S.bits()[MAX_WORDS + l] = x;
-    S.bits()[2 * MAX_WORDS + l] = (l == 0) ? 1u : 0u;
     for (uint32_t i = l; i < n; i += 32) {
         if (i >= hop && i < hop + keep) S.c2()[i - hop] = (uint16_t)i;
         S.t1()[i] = 0;
@@ -150,9 +249,11 @@ __device__ void ks_start(const SearchParams& sp, const KsSlot& S, uint32_t r, ui
 }
 
 // upperBoundK2 (src:1002-1020): every P member keeps neiInG + k >= q, neiInG over P ∪ C1.
-__device__ bool ks_upper_bound(const SearchParams& sp, const RootView& R, const KsSlot& S, uint32_t np, uint32_t PC1w) {
+template <int NW>
+__device__ bool ks_upper_bound(const SearchParams& sp, const RootView& R, const KsSlot<NW>& S, uint32_t np,
+                               const Bits<NW>& PC1) {
     const unsigned l = lane_id();
-    S.mask()[l] = PC1w;
+    bits_store(S.mask(), PC1);
     __syncwarp();
     bool ok = true;
     for (uint32_t i = l; i < np; i += 32) {
@@ -164,31 +265,37 @@ __device__ bool ks_upper_bound(const SearchParams& sp, const RootView& R, const 
     return ok;
 }
 
+template <int NW>
 struct Emitted {
     uint32_t np, nc, nx;
-    uint32_t Pw, Cw, Xw;   // this lane's word
+    Bits<NW> P, C, X;   // this lane's words
 };
 
 // Runs the k-search state machine (src:1993-2442) of the root held in S until
 // it emits one task (returns 1, task in *e) or the root is finished (returns 0).
 // The frame bookkeeping after an emission is done before returning, so the
 // saved state resumes exactly where the reference resumes after its pause.
-__device__ int ks_advance(const SearchParams& sp, const KsSlot& S, Emitted* e) {
+template <int NW>
+__device__ int ks_advance(const SearchParams& sp, const KsSlot<NW>& S, Emitted<NW>* e) {
     const unsigned l = lane_id();
     const uint32_t r = S.root();
     const RootView R = root_view(sp, r);
     const int k = R.k, q = R.q;
     const uint32_t n = R.n, W = R.W;
-    uint32_t C1w = S.bits()[l], Xw = S.bits()[MAX_WORDS + l], Pw = S.bits()[2 * MAX_WORDS + l];
+    Bits<NW> C1 = bits_load<NW>(S.c1bits(), S.BW), X = bits_load<NW>(S.xbits(), S.BW), P = bits_load<NW>(S.pbits(), S.BW);
     uint32_t sz = S.sz(), np = S.np(), nc2 = S.nc2();
     int emitted = 0;
-    uint32_t emitC = 0;
+    Bits<NW> emitC = bits_zero<NW>();
 
     auto update13 = [&](uint32_t node, uint16_t tag) {   // updateCand13, src:1042-1097
-        const uint32_t m2 = (l < W) ? __ldg(R.M2 + (uint64_t)node * W + l) : 0u;
-        uint32_t drop = C1w & ~m2;
-        C1w &= m2;
-        while (drop) { const int b = __ffs(drop) - 1; S.t1()[l * 32 + b] = tag; drop &= drop - 1; }
+#pragma unroll
+        for (int j = 0; j < NW; ++j) {
+            const uint32_t wi = l + 32u * j;
+            const uint32_t m2 = (wi < W) ? __ldg(R.M2 + (uint64_t)node * W + wi) : 0u;
+            uint32_t drop = C1.w[j] & ~m2;
+            C1.w[j] &= m2;
+            while (drop) { const int b = __ffs(drop) - 1; S.t1()[wi * 32 + b] = tag; drop &= drop - 1; }
+        }
     };
     auto update23 = [&](uint32_t node, uint16_t tag) {   // updateCand23, src:1099-1122 (order preserving)
         const uint32_t* m2row = R.M2 + (uint64_t)node * W;
@@ -212,7 +319,7 @@ __device__ int ks_advance(const SearchParams& sp, const KsSlot& S, Emitted* e) {
     auto include = [&](uint32_t u) {
         if (l == 0) S.P()[np] = u;
         ++np;
-        if (l == (u >> 5)) Pw |= 1u << (u & 31);
+        bits_set(P, u);
         __syncwarp();
     };
     auto c2_pop = [&]() -> uint32_t { --nc2; return S.c2()[nc2]; };
@@ -220,10 +327,10 @@ __device__ int ks_advance(const SearchParams& sp, const KsSlot& S, Emitted* e) {
     auto setfr = [&](uint32_t f, uint32_t val) { __syncwarp(); if (l == 0) S.fr()[f] = val; __syncwarp(); };
 
     while (sz && !emitted) {
-        if (sz + S.w[4] >= (uint32_t)KS_MAX_DEPTH) {
-            // src:1987-1991: the reference abandons the rest of the root at this depth; with
-            // the root split into jobs that cut is not reproducible, so the run reports it
-            if (l == 0) { atomicAdd(&sp.ctr->depth_capped, 1u); raise_error(sp.ctr, KPLEX_ERR_CAPACITY); }
+        if (sz + 1 >= S.L.c2 - S.L.fr) {
+            // a frame stack sized n_max + 8 cannot fill (see KS_MAX_DEPTH); guard the
+            // shared-memory layout all the same
+            if (l == 0) { atomicAdd(&sp.ctr->depth_capped, 1u); raise_error(sp.ctr, KPLEX_ERR_INTERNAL); }
             sz = 0;
             break;
         }
@@ -233,15 +340,15 @@ __device__ int ks_advance(const SearchParams& sp, const KsSlot& S, Emitted* e) {
         const uint32_t res = fr_res(F), br = fr_br(F), st = fr_st(F);
         if (st == 0) {
             if (nc2 == 0) {   // leaf: emit (P, C1, X) (src:2005-2092)
-                const int nc1 = warp_sum(__popc(C1w));
+                const int nc1 = bits_count(C1);
                 bool ok = (int)np + nc1 >= q;
-                if (ok && np > 1) ok = ks_upper_bound(sp, R, S, np, Pw | C1w);
+                if (ok && np > 1) ok = ks_upper_bound(sp, R, S, np, bits_or(P, C1));
                 --sz;
-                if (ok) { emitted = 1; emitC = C1w; }
+                if (ok) { emitted = 1; emitC = C1; }
                 continue;
             }
             const uint32_t u = c2_pop();   // exclude the last C2 vertex first
-            if (l == (u >> 5)) Xw |= 1u << (u & 31);
+            bits_set(X, u);
             setfr(f, fr_pack(res, br, 1, u));
             setfr(sz, fr_pack(res, 1, 0, 0));
             ++sz;
@@ -250,7 +357,7 @@ __device__ int ks_advance(const SearchParams& sp, const KsSlot& S, Emitted* e) {
         if (st == 1 || st == 3) {   // child returned: the excluded vertex goes back to C2's end
             const uint32_t u = fr_v(F);
             c2_push(u);
-            if (l == (u >> 5)) Xw &= ~(1u << (u & 31));
+            bits_clear(X, u);
             setfr(f, fr_pack(res, st == 3 ? br + 1 : br, 2, u));
             continue;
         }
@@ -262,7 +369,7 @@ __device__ int ks_advance(const SearchParams& sp, const KsSlot& S, Emitted* e) {
                 update23(u, tag);
                 if (nc2) {
                     const uint32_t w = c2_pop();
-                    if (l == (w >> 5)) Xw |= 1u << (w & 31);
+                    bits_set(X, w);
                     setfr(f, fr_pack(res, br, 3, w));
                 } else {
                     setfr(f, fr_pack(res, br, 4, 0));
@@ -280,19 +387,19 @@ __device__ int ks_advance(const SearchParams& sp, const KsSlot& S, Emitted* e) {
                 const uint32_t u = c2_pop();
                 include(u);
                 update13(u, tag);
-                const int nc1 = warp_sum(__popc(C1w));
+                const int nc1 = bits_count(C1);
                 if ((int)np + nc1 < q) continue;
-                if (np > 1 && !ks_upper_bound(sp, R, S, np, Pw | C1w)) continue;
+                if (np > 1 && !ks_upper_bound(sp, R, S, np, bits_or(P, C1))) continue;
                 // isKplex2 (src:568-584): c stays if P + c is a k-plex
-                S.mask()[l] = Pw;
-                S.aux()[l] = 0u;
-                S.keep()[l] = 0u;
+                bits_store(S.mask(), P);
+                bits_fill<NW>(S.aux(), 0u);
+                bits_fill<NW>(S.keep(), 0u);
                 __syncwarp();
                 for (uint32_t i = l; i < np; i += 32) {
                     const uint32_t v = S.P()[i];
                     if (row_and_popc(R.A + (uint64_t)v * W, S.mask(), W) + k == (int)np) atomicOr(&S.aux()[v >> 5], 1u << (v & 31));
                 }
-                const int m1 = bits_to_list(C1w, S.lst());
+                const int m1 = bits_list(C1, S.lst());
                 for (int i = l; i < m1; i += 32) {
                     const uint32_t v = S.lst()[i];
                     const uint32_t* row = R.A + (uint64_t)v * W;
@@ -302,7 +409,7 @@ __device__ int ks_advance(const SearchParams& sp, const KsSlot& S, Emitted* e) {
                 }
                 __syncwarp();
                 emitted = 1;
-                emitC = S.keep()[l];
+                emitC = bits_load<NW>(S.keep(), S.BW);
                 continue;
             }
             continue;
@@ -311,7 +418,7 @@ __device__ int ks_advance(const SearchParams& sp, const KsSlot& S, Emitted* e) {
         for (uint32_t i = 0; i < br; ++i) {
             const uint32_t node = S.P()[np - 1];
             --np;
-            if (l == (node >> 5)) Pw &= ~(1u << (node & 31));
+            bits_clear(P, node);
             c2_push(node);
         }
         for (uint32_t b = 0; b < n; b += 32) {
@@ -321,7 +428,7 @@ __device__ int ks_advance(const SearchParams& sp, const KsSlot& S, Emitted* e) {
             const unsigned m1 = __ballot_sync(FULL, h1), m2 = __ballot_sync(FULL, h2);
             if (h1) S.t1()[i] = 0;
             if (h2) { S.t2()[i] = 0; S.c2()[nc2 + __popc(m2 & ((1u << l) - 1))] = (uint16_t)i; }
-            if (l == (b >> 5)) C1w |= m1;
+            bits_or_word(C1, b >> 5, m1);
             nc2 += __popc(m2);
             __syncwarp();
         }
@@ -329,14 +436,14 @@ __device__ int ks_advance(const SearchParams& sp, const KsSlot& S, Emitted* e) {
     }
     if (emitted) {
         e->np = np;
-        e->nc = (uint32_t)warp_sum(__popc(emitC));
-        e->nx = (uint32_t)warp_sum(__popc(Xw));
-        e->Pw = Pw; e->Cw = emitC; e->Xw = Xw;
+        e->nc = (uint32_t)bits_count(emitC);
+        e->nx = (uint32_t)bits_count(X);
+        e->P = P; e->C = emitC; e->X = X;
     }
     __syncwarp();
-    S.bits()[l] = C1w;
-    S.bits()[MAX_WORDS + l] = Xw;
-    S.bits()[2 * MAX_WORDS + l] = Pw;
+    bits_store(S.c1bits(), C1);
+    bits_store(S.xbits(), X);
+    bits_store(S.pbits(), P);
     if (l == 0) { S.sz() = sz; S.np() = np; S.nc2() = nc2; }
     __syncwarp();
     return emitted;
@@ -400,9 +507,10 @@ __device__ __forceinline__ void rowg_popc2(const uint32_t* row, const uint32_t* 
     c2 = a2;
 }
 
+// Per-warp shared memory of the branch-and-bound, bitsets of BW = 32 * NW words.
 struct BnbSmem {
     uint32_t* rec;    // slot_words: record being loaded from the pool
-    uint32_t* P;      // 32 words each
+    uint32_t* P;      // BW words each
     uint32_t* PC;
     uint32_t* SAT;
     uint32_t* ROW;
@@ -429,28 +537,31 @@ __host__ __device__ inline uint32_t stack_cache_words(uint32_t slot_words) {
     return (STACK_CACHE * slot_words + STACK_CACHE + 3u) & ~3u;
 }
 
-__host__ __device__ inline uint32_t bnb_smem_words(uint32_t nmax, uint32_t slot_words, uint32_t a_words) {
-    const uint32_t lists = 3 * ((nmax + 1) / 2);
-    return (((slot_words + 9 * MAX_WORDS + lists) + 3u) & ~3u) + 32u + stack_cache_words(slot_words) + a_words;
+__host__ __device__ inline uint32_t bnb_fixed_words(uint32_t nmax, uint32_t slot_words, uint32_t bw) {
+    return ((slot_words + 9 * bw + 3 * ((nmax + 1) / 2)) + 3u) & ~3u;
 }
 
-__device__ inline BnbSmem bnb_smem(uint32_t* base, uint32_t nmax, uint32_t slot_words) {
+__host__ __device__ inline uint32_t bnb_smem_words(uint32_t nmax, uint32_t slot_words, uint32_t a_words, uint32_t bw) {
+    return bnb_fixed_words(nmax, slot_words, bw) + 32u + stack_cache_words(slot_words) + a_words;
+}
+
+__device__ inline BnbSmem bnb_smem(uint32_t* base, uint32_t nmax, uint32_t slot_words, uint32_t bw) {
     BnbSmem m;
     uint32_t* p = base;
     m.rec = p; p += slot_words;
-    m.P = p; p += MAX_WORDS;
-    m.PC = p; p += MAX_WORDS;
-    m.SAT = p; p += MAX_WORDS;
-    m.ROW = p; p += MAX_WORDS;
-    m.M2 = p; p += MAX_WORDS;
-    m.M4 = p; p += MAX_WORDS;
-    m.NC = p; p += MAX_WORDS;
-    m.NX = p; p += MAX_WORDS;
-    m.SB = p; p += MAX_WORDS;
+    m.P = p; p += bw;
+    m.PC = p; p += bw;
+    m.SAT = p; p += bw;
+    m.ROW = p; p += bw;
+    m.M2 = p; p += bw;
+    m.M4 = p; p += bw;
+    m.NC = p; p += bw;
+    m.NX = p; p += bw;
+    m.SB = p; p += bw;
     m.list = reinterpret_cast<uint16_t*>(p); p += (nmax + 1) / 2;
     m.gv = reinterpret_cast<uint16_t*>(p); p += (nmax + 1) / 2;
     m.pv = reinterpret_cast<uint16_t*>(p); p += (nmax + 1) / 2;
-    m.CT = reinterpret_cast<unsigned long long*>(base + (((slot_words + 9 * MAX_WORDS + 3 * ((nmax + 1) / 2)) + 3u) & ~3u));
+    m.CT = reinterpret_cast<unsigned long long*>(base + bnb_fixed_words(nmax, slot_words, bw));
     m.SCT = reinterpret_cast<uint32_t*>(m.CT + 16);
     m.SC = m.SCT + STACK_CACHE;
     m.A = m.SCT + stack_cache_words(slot_words);
@@ -529,36 +640,43 @@ __device__ bool left_maximal(const SearchParams& sp, const RootView& R, const Bn
 }
 
 // Adds one maximal k-plex (list[0..s)) to the count and hash.
+template <int NW>
 __device__ void emit_plex(const SearchParams& sp, const RootView& R, const BnbSmem& m, int s,
                           unsigned long long& cnt, unsigned long long& hsum) {
     const unsigned l = lane_id();
     if (l == 0) ++cnt;
     if (!sp.hash_on) return;
-    m.SB[l] = 0u;
+    bits_fill<NW>(m.SB, 0u);
     __syncwarp();
     for (int i = l; i < s; i += 32) {
         const uint32_t rk = __ldg(R.srank + m.list[i]);
         atomicOr(&m.SB[rk >> 5], 1u << (rk & 31));
     }
     __syncwarp();
-    uint32_t w = m.SB[l];
+    // the sorted original ids, word by word in ascending order: lane L walks word
+    // 32 j + L and passes the running hash on to lane L + 1
     uint64_t x = plex_hash_begin((uint32_t)s);
-    for (int L = 0; L < 32; ++L) {
-        if ((int)l == L) {
-            while (w) {
-                const int b = __ffs(w) - 1;
-                w &= w - 1;
-                x = plex_hash_step(x, __ldg(R.sorig + L * 32 + b));
+#pragma unroll
+    for (int j = 0; j < NW; ++j) {
+        uint32_t w = m.SB[32 * j + l];
+        for (int L = 0; L < 32; ++L) {
+            if ((int)l == L) {
+                while (w) {
+                    const int b = __ffs(w) - 1;
+                    w &= w - 1;
+                    x = plex_hash_step(x, __ldg(R.sorig + (32 * j + L) * 32 + b));
+                }
             }
+            x = __shfl_sync(FULL, x, L);
         }
-        x = __shfl_sync(FULL, x, L);
     }
     if (l == 0) hsum += x;
 }
 
+template <int NW>
 struct Node {
     uint32_t root, np, nc, nx;
-    uint32_t Pw, Cw, Xw;   // this lane's word of each bitset
+    Bits<NW> P, C, X;   // this lane's words of each bitset
 };
 
 // Counters live in the warp's shared memory (m.CT) and are updated by lane 0.
@@ -577,18 +695,20 @@ struct WarpWork {
 // One branch-and-bound node (BNB, src:1516-1724).  Returns true when the node
 // produced an include child, which is left in *t; the exclude child is pushed
 // on the warp's stack.
-__device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootView& R, const uint32_t* A, Node* t, WarpWork& ww) {
+template <int NW>
+__device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootView& R, const uint32_t* A, Node<NW>* t,
+                         WarpWork& ww) {
     const unsigned l = lane_id();
     const int k = R.k, q = R.q;
     const uint32_t W = R.W, Wt = sp.Wt, SW = sp.slot_words;
     const uint32_t np = t->np, nc = t->nc, nx = t->nx;
-    const uint32_t Pw = t->Pw, Cw = t->Cw, Xw = t->Xw;
+    const Bits<NW> P = t->P, C = t->C, X = t->X;
     if ((int)(np + nc) < q) return false;
-    m.P[l] = Pw;
-    m.PC[l] = Pw | Cw;
+    bits_store(m.P, P);
+    bits_store(m.PC, bits_or(P, C));
     __syncwarp();
-    bits_to_list(Pw, m.list);
-    bits_to_list(Cw, m.list + np);
+    bits_list(P, m.list);
+    bits_list(C, m.list + np);
     const int tot = (int)(np + nc);
     for (int i = l; i < tot; i += 32) {
         int g, p;
@@ -600,7 +720,7 @@ __device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootVie
     __syncwarp();
     if (nc == 0) {   // src:1579-1588
         if (nx == 0 && (int)np >= q && left_maximal(sp, R, m, (int)np, m.pv, m.P, ww.bb))
-            emit_plex(sp, R, m, (int)np, ww.cnt, ww.hsum);
+            emit_plex<NW>(sp, R, m, (int)np, ww.cnt, ww.hsum);
         return false;
     }
     // pivot in P: minimum neiInG, ties to the smaller index (src:1592-1620)
@@ -620,7 +740,7 @@ __device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootVie
     int piv, pmin, pval, pidx;
     if (minP + k < tot) {
         // candidates not adjacent to the P pivot (src:1626-1663)
-        m.ROW[l] = (l < W) ? A[(uint32_t)pp * W + l] : 0u;
+        bits_store(m.ROW, bits_load<NW>(A + (uint32_t)pp * W, W));
         __syncwarp();
         pmin = INT_MAX; piv = -1; pval = 0; pidx = -1;
         for (int i = l; i < (int)nc; i += 32) {
@@ -644,10 +764,10 @@ __device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootVie
         if (pmin >= tot - k) {
             // P ∪ C is a k-plex (src:1698-1717)
             if (tot < q) return false;
-            const int nxl = bits_to_list(Xw, m.list + tot);
+            const int nxl = bits_list(X, m.list + tot);
             for (int i = l; i < nxl; i += 32)
                 m.gv[tot + i] = (uint16_t)rowg_popc(A + (uint32_t)m.list[tot + i] * W, m.PC, W);
-            m.SAT[l] = 0u;
+            bits_fill<NW>(m.SAT, 0u);
             __syncwarp();
             for (int i = l; i < tot; i += 32)
                 if ((int)m.gv[i] + k == tot) { const uint32_t u = m.list[i]; atomicOr(&m.SAT[u >> 5], 1u << (u & 31)); }
@@ -659,28 +779,32 @@ __device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootVie
             }
             if (l == 0) ww.bb += (unsigned long long)nxl * 4ull * W;
             if (__any_sync(FULL, ext)) return false;
-            if (left_maximal(sp, R, m, tot, m.gv, m.PC, ww.bb)) emit_plex(sp, R, m, tot, ww.cnt, ww.hsum);
+            if (left_maximal(sp, R, m, tot, m.gv, m.PC, ww.bb)) emit_plex<NW>(sp, R, m, tot, ww.cnt, ww.hsum);
             return false;
         }
     }
     // ---------------- branch on piv (src:1197-1465)
     if (piv < 0 || pidx < 0) { if (l == 0) raise_error(sp.ctr, KPLEX_ERR_INTERNAL); return false; }
     const uint32_t v = (uint32_t)piv;
-    const uint32_t vw = v >> 5, vb = 1u << (v & 31);
     {   // exclude child -> this warp's stack
         if (ww.stop - ww.sbot >= sp.stack_depth) { if (l == 0) raise_error(sp.ctr, KPLEX_ERR_INTERNAL); return false; }
         uint32_t* dst = ww.stack + (ww.stop % sp.stack_depth) * SW;
-        const uint32_t Cx = (l == vw) ? (Cw & ~vb) : Cw;
-        const uint32_t Xx = (l == vw) ? (Xw | vb) : Xw;
+        Bits<NW> Cx = C, Xx = X;
+        bits_clear(Cx, v);
+        bits_set(Xx, v);
         uint32_t* cdst = m.SC + (uint32_t)(ww.stop % STACK_CACHE) * SW;   // shared-memory copy
         if (l == 0) {
             __stcg(dst + 0, t->root); __stcg(dst + 1, np | ((nc - 1) << 16)); __stcg(dst + 2, nx + 1); __stcg(dst + 3, 0u);
             cdst[0] = t->root; cdst[1] = np | ((nc - 1) << 16); cdst[2] = nx + 1; cdst[3] = 0u;
             m.SCT[ww.stop % STACK_CACHE] = (uint32_t)ww.stop;
         }
-        if (l < Wt) {
-            __stcg(dst + 4 + l, Pw); __stcg(dst + 4 + Wt + l, Cx); __stcg(dst + 4 + 2 * Wt + l, Xx);
-            cdst[4 + l] = Pw; cdst[4 + Wt + l] = Cx; cdst[4 + 2 * Wt + l] = Xx;
+#pragma unroll
+        for (int j = 0; j < NW; ++j) {
+            const uint32_t wi = l + 32u * j;
+            if (wi < Wt) {
+                __stcg(dst + 4 + wi, P.w[j]); __stcg(dst + 4 + Wt + wi, Cx.w[j]); __stcg(dst + 4 + 2 * Wt + wi, Xx.w[j]);
+                cdst[4 + wi] = P.w[j]; cdst[4 + Wt + wi] = Cx.w[j]; cdst[4 + 2 * Wt + wi] = Xx.w[j];
+            }
         }
         __syncwarp();
         ++ww.stop;
@@ -688,13 +812,14 @@ __device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootVie
     }
     // include child
     const uint32_t np1 = np + 1;
-    const uint32_t P1 = (l == vw) ? (Pw | vb) : Pw;
-    m.ROW[l] = (l < W) ? A[v * W + l] : 0u;
-    m.M2[l] = (l < W) ? __ldg(R.M2 + (uint64_t)v * W + l) : 0u;
-    m.M4[l] = (l < W) ? __ldg(R.M4 + (uint64_t)v * W + l) : 0u;
-    m.SAT[l] = 0u;
-    m.NC[l] = 0u;
-    m.NX[l] = 0u;
+    Bits<NW> P1 = P;
+    bits_set(P1, v);
+    bits_store(m.ROW, bits_load<NW>(A + v * W, W));
+    bits_store(m.M2, bits_ldg<NW>(R.M2 + (uint64_t)v * W, W));
+    bits_store(m.M4, bits_ldg<NW>(R.M4 + (uint64_t)v * W, W));
+    bits_fill<NW>(m.SAT, 0u);
+    bits_fill<NW>(m.NC, 0u);
+    bits_fill<NW>(m.NX, 0u);
     __syncwarp();
     // saturated members of P + v: neiInP' + k == |P'|
     for (int i = l; i < (int)np; i += 32) {
@@ -702,8 +827,8 @@ __device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootVie
         const int pu = (int)m.pv[i] + (int)test_bit(m.ROW, u);
         if (pu + k == (int)np1) atomicOr(&m.SAT[u >> 5], 1u << (u & 31));
     }
-    if (l == 0 && (int)m.pv[pidx] + k == (int)np1) atomicOr(&m.SAT[vw], vb);
-    m.P[l] = P1;
+    if (l == 0 && (int)m.pv[pidx] + k == (int)np1) atomicOr(&m.SAT[v >> 5], 1u << (v & 31));
+    bits_store(m.P, P1);
     __syncwarp();
     // C filter: class >= UNLINK2EQUAL and P' + c a k-plex (isKplex3)
     for (int i = l; i < (int)nc; i += 32) {
@@ -715,9 +840,9 @@ __device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootVie
     }
     if (l == 0) ww.bb += (unsigned long long)nc * 4ull * W;
     __syncwarp();
-    const uint32_t C1 = m.NC[l];
-    const uint32_t nc1 = (uint32_t)warp_sum(__popc(C1));
-    m.PC[l] = P1 | C1;
+    const Bits<NW> C1 = bits_load<NW>(m.NC, 32 * NW);
+    const uint32_t nc1 = (uint32_t)bits_count(C1);
+    bits_store(m.PC, bits_or(P1, C1));
     __syncwarp();
     // upperBound2 over P' (src:1022-1040)
     bool ub = true;
@@ -728,7 +853,7 @@ __device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootVie
     if (l == 0) ww.bb += (unsigned long long)np1 * 4ull * W;
     if (!__all_sync(FULL, ub)) return false;
     // X filter: class >= UNLINK2MORE and P' + x a k-plex
-    const int nxl = bits_to_list(Xw, m.list);
+    const int nxl = bits_list(X, m.list);
     for (int i = l; i < nxl; i += 32) {
         const uint32_t x = m.list[i];
         if (!test_bit(m.M4, x)) continue;
@@ -738,30 +863,39 @@ __device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootVie
     }
     if (l == 0) ww.bb += (unsigned long long)nxl * 4ull * W;
     __syncwarp();
-    const uint32_t X1 = m.NX[l];
-    t->nx = (uint32_t)warp_sum(__popc(X1));
-    t->Pw = P1; t->Cw = C1; t->Xw = X1;
+    const Bits<NW> X1 = bits_load<NW>(m.NX, 32 * NW);
+    t->nx = (uint32_t)bits_count(X1);
+    t->P = P1; t->C = C1; t->X = X1;
     t->np = np1; t->nc = nc1;
     if (l == 0) { ++ww.tasks; ww.bb += 12ull * W; }
     return true;
 }
 
 // ============================================================== the persistent kernel
-__device__ __forceinline__ void load_record(const uint32_t* src, uint32_t Wt, Node* t, bool cg) {
+template <int NW>
+__device__ __forceinline__ void load_record(const uint32_t* src, uint32_t Wt, Node<NW>* t, bool cg) {
     const unsigned l = lane_id();
     if (cg) {
         t->root = __ldcg(src);
         const uint32_t h1 = __ldcg(src + 1);
         t->np = h1 & 0xffff; t->nc = h1 >> 16; t->nx = __ldcg(src + 2);
-        t->Pw = (l < Wt) ? __ldcg(src + 4 + l) : 0u;
-        t->Cw = (l < Wt) ? __ldcg(src + 4 + Wt + l) : 0u;
-        t->Xw = (l < Wt) ? __ldcg(src + 4 + 2 * Wt + l) : 0u;
+#pragma unroll
+        for (int j = 0; j < NW; ++j) {
+            const uint32_t wi = l + 32u * j;
+            t->P.w[j] = (wi < Wt) ? __ldcg(src + 4 + wi) : 0u;
+            t->C.w[j] = (wi < Wt) ? __ldcg(src + 4 + Wt + wi) : 0u;
+            t->X.w[j] = (wi < Wt) ? __ldcg(src + 4 + 2 * Wt + wi) : 0u;
+        }
     } else {
         t->root = src[0];
         t->np = src[1] & 0xffff; t->nc = src[1] >> 16; t->nx = src[2];
-        t->Pw = (l < Wt) ? src[4 + l] : 0u;
-        t->Cw = (l < Wt) ? src[4 + Wt + l] : 0u;
-        t->Xw = (l < Wt) ? src[4 + 2 * Wt + l] : 0u;
+#pragma unroll
+        for (int j = 0; j < NW; ++j) {
+            const uint32_t wi = l + 32u * j;
+            t->P.w[j] = (wi < Wt) ? src[4 + wi] : 0u;
+            t->C.w[j] = (wi < Wt) ? src[4 + Wt + wi] : 0u;
+            t->X.w[j] = (wi < Wt) ? src[4 + 2 * Wt + wi] : 0u;
+        }
     }
 }
 
@@ -854,7 +988,9 @@ __device__ bool bq_pop(const BlockQueue& q, uint32_t* dst) {
     return true;
 }
 
+template <int NW>
 __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
+    constexpr uint32_t BW = 32 * NW;
     extern __shared__ uint4 smem4[];
     uint32_t* smem = reinterpret_cast<uint32_t*>(smem4);
     const unsigned l = lane_id();
@@ -862,10 +998,10 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
     const unsigned warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t SW = sp.slot_words, Wt = sp.Wt;
     const bool producer = (wib == 0);
-    const KsLayout KL = ks_layout(nmax);
-    const KsSlot S{smem, KL};
+    const KsLayout KL = ks_layout(nmax, NW);
+    const KsSlot<NW> S{smem, KL};
     const BlockQueue BQ{smem + KL.total, SW};
-    const BnbSmem m = bnb_smem(smem + KL.total + bq_words(SW) + wib * bnb_smem_words(nmax, SW, sp.a_words), nmax, SW);
+    const BnbSmem m = bnb_smem(smem + KL.total + bq_words(SW) + wib * bnb_smem_words(nmax, SW, sp.a_words, BW), nmax, SW, BW);
     if (threadIdx.x < BQ_HDR) BQ.w[threadIdx.x] = 0u;
     __syncthreads();
     const uint32_t* A = nullptr;
@@ -886,18 +1022,18 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
         if (is_idle) { if (l == 0) atomicSub(BQ.idle(), 1u); is_idle = false; }
         spins = 0;
     };
-    Node t{};
+    Node<NW> t{};
     uint32_t cur_root = 0xffffffffu;
     RootView R{};
-    Emitted e{};
+    Emitted<NW> e{};
 
     for (;;) {
         // ---------------- local depth-first work
         if (!have && ww.stop > ww.sbot) {
             --ww.stop;
             const uint32_t cs = (uint32_t)(ww.stop % STACK_CACHE);
-            if (m.SCT[cs] == (uint32_t)ww.stop) load_record(m.SC + cs * SW, Wt, &t, false);   // still cached
-            else load_record(ww.stack + (ww.stop % sp.stack_depth) * SW, Wt, &t, true);
+            if (m.SCT[cs] == (uint32_t)ww.stop) load_record<NW>(m.SC + cs * SW, Wt, &t, false);   // still cached
+            else load_record<NW>(ww.stack + (ww.stop % sp.stack_depth) * SW, Wt, &t, true);
             have = true;
             __syncwarp();
         }
@@ -945,7 +1081,7 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
             }
             if (l == 0) ++ww.nodes;
             const long long b0 = clock64();
-            have = bnb_node(sp, m, R, A, &t, ww);
+            have = bnb_node<NW>(sp, m, R, A, &t, ww);
             __syncwarp();
             if (l == 0) CT[CT_BNB_CYC] += (unsigned long long)(clock64() - b0);
             if (!have && ww.stop == ww.sbot) {
@@ -989,20 +1125,20 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
                         uint32_t lo2 = 0, hi2 = sp.nroots;
                         while (hi2 - lo2 > 1) { const uint32_t mid = (lo2 + hi2) >> 1; if (__ldg(sp.job_base + mid) <= (uint32_t)j) lo2 = mid; else hi2 = mid; }
                         const RootDesc rd = sp.roots[lo2];
-                        ks_start(sp, S, lo2, (uint32_t)j - __ldg(sp.job_base + lo2), rd);
+                        ks_start<NW>(sp, S, lo2, (uint32_t)j - __ldg(sp.job_base + lo2), rd);
                         ks_active = true;
                         wake();
                     }
                 }
                 if (ks_active) {
                     const long long c0 = clock64();
-                    const int got = ks_advance(sp, S, &e);
+                    const int got = ks_advance<NW>(sp, S, &e);
                     if (l == 0) CT[CT_KS_CYC] += (unsigned long long)(clock64() - c0);
                     if (got) {
                         if (l == 0) ++CT[CT_KS_TASKS];
                         const uint32_t r = S.root();
                         // stage this lane's words in shared memory; the record is hdr | P | C | X
-                        m.P[l] = e.Pw; m.NC[l] = e.Cw; m.NX[l] = e.Xw;
+                        bits_store(m.P, e.P); bits_store(m.NC, e.C); bits_store(m.NX, e.X);
                         __syncwarp();
                         auto word = [&](unsigned i) -> uint32_t {
                             if (i == 0) return r;
@@ -1025,7 +1161,7 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
                         if (!pushed) pushed = pool_push(sp, word);
                         if (!pushed) {   // ring full: keep the task
                             t.root = r; t.np = e.np; t.nc = e.nc; t.nx = e.nx;
-                            t.Pw = e.Pw; t.Cw = e.Cw; t.Xw = e.Xw;
+                            t.P = e.P; t.C = e.C; t.X = e.X;
                             have = true;
                             wake();
                             if (!counted) { if (l == 0) atomicAdd(&sp.ctr->holders, 1u); counted = true; }
@@ -1051,7 +1187,7 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
         if (!is_idle) { if (l == 0) atomicAdd(BQ.idle(), 1u); is_idle = true; }
         if (bq_pop(BQ, m.rec)) {   // takes over the record's unit of work
             wake();
-            load_record(m.rec, Wt, &t, false);
+            load_record<NW>(m.rec, Wt, &t, false);
             have = true;
             counted = true;
             if (l == 0) atomicAdd(&sp.ctr->holders, 1u);
@@ -1072,7 +1208,7 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
                 if (got) {
                     wake();
                     if (which == 2 && l == 0) ++CT[CT_REFILL];
-                    load_record(m.rec, Wt, &t, false);
+                    load_record<NW>(m.rec, Wt, &t, false);
                     have = true;
                     counted = true;
                     if (l == 0) atomicAdd(&sp.ctr->holders, 1u);
@@ -1129,12 +1265,23 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
     }
 }
 
-// One body, compiled for two register budgets: 3 blocks of 256 threads per SM
-// (80 registers, some spills) or 2 blocks (up to 128 registers).
-__global__ void __launch_bounds__(256, 3) search_kernel_3(SearchParams sp, uint32_t nmax) { search_body(sp, nmax); }
-__global__ void __launch_bounds__(256, 2) search_kernel_2(SearchParams sp, uint32_t nmax) { search_body(sp, nmax); }
+// One body, compiled per bitset width (NW words per lane) and register budget:
+// MINB blocks of 256 threads per SM (2: up to 128 registers; 3: 80, with some
+// spills).  Roots above 1024 vertices need NW = 2, built for 2 blocks only.
+template <int NW, int MINB>
+__global__ void __launch_bounds__(256, MINB) search_kernel(SearchParams sp, uint32_t nmax) { search_body<NW>(sp, nmax); }
 
-uint32_t bnb_smem_words_host(uint32_t nmax, uint32_t slot_words, uint32_t a_words) { return bnb_smem_words(nmax, slot_words, a_words); }
-uint32_t ks_slot_words_host(uint32_t nmax, uint32_t slot_words) { return ks_layout(nmax).total + bq_words(slot_words); }
+SearchKernel search_kernel_for(uint32_t nw, int minb) {
+    if (nw > 1) return search_kernel<2, 2>;
+    return minb == 3 ? search_kernel<1, 3> : search_kernel<1, 2>;
+}
+
+uint32_t search_words_per_lane(uint32_t max_w) { return max_w > 32 ? 2u : 1u; }
+uint32_t bnb_smem_words_host(uint32_t nmax, uint32_t slot_words, uint32_t a_words, uint32_t nw) {
+    return bnb_smem_words(nmax, slot_words, a_words, 32 * nw);
+}
+uint32_t ks_slot_words_host(uint32_t nmax, uint32_t slot_words, uint32_t nw) {
+    return ks_layout(nmax, nw).total + bq_words(slot_words);
+}
 
 }  // namespace kplex

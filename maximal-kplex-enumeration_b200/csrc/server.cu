@@ -44,7 +44,7 @@ struct Request {
 
 // Device bytes a request adds while in flight: its pruned CSR and vertex maps
 // (bounded by the input's), its result slots, and the decomposition arena of
-// its roots, bounded per root by a local subgraph of min(degree + 1, 1024)
+// its roots, bounded per root by a local subgraph of min(degree + 1, MAX_LOCAL)
 // vertices holding three adjacency-sized bit matrices and the id tables.
 static uint64_t estimate_request_bytes(const Request& r) {
     const uint64_t m = r.adj.size();

@@ -36,9 +36,10 @@ __device__ __forceinline__ int warp_excl_scan(int v, int* total) {
     return x - v;
 }
 
-// Lane l holds word l of a bitset (0 beyond its length).  Writes the set
-// bits' indices in ascending order to list[0..) and returns their count.
-__device__ __forceinline__ int bits_to_list(unsigned w, uint16_t* list) {
+// Lane l holds word l of a 32-word group of a bitset whose first bit is
+// `base` (0 beyond its length).  Writes the set bits' indices in ascending
+// order to list[0..) and returns their count.
+__device__ __forceinline__ int bits_to_list(unsigned w, uint16_t* list, unsigned base = 0) {
     // words are visited in order (only the non-zero ones); within a word every
     // lane tests one bit, so all 32 lanes stay active however dense the word is
     const unsigned l = lane_id();
@@ -48,7 +49,7 @@ __device__ __forceinline__ int bits_to_list(unsigned w, uint16_t* list) {
         const int j = __ffs(nz) - 1;
         nz &= nz - 1;
         const unsigned word = __shfl_sync(FULL, w, j);
-        if ((word >> l) & 1u) list[off + __popc(word & ((1u << l) - 1u))] = (uint16_t)(j * 32 + l);
+        if ((word >> l) & 1u) list[off + __popc(word & ((1u << l) - 1u))] = (uint16_t)(base + j * 32 + l);
         off += __popc(word);
     }
     __syncwarp();

@@ -83,7 +83,13 @@ static const int REF_BLK = 1024;
 // device build accept up to 2048 local vertices and left sets up to 8192.
 static const int MAX_LOCAL = 2048;
 static const int MAX_LEFT = 8192;
-static const int MAX_DEPTH = 1000; // common.h:15
+// The reference's k-search stack holds MAX_DEPTH = 1000 frames (common.h:15) and
+// abandons the rest of a root when it would go deeper (src:1987-1991), which
+// loses results on roots with about 1000 or more C2 vertices.  A path pushes at
+// most one frame per C2 vertex plus a leaf frame, so a stack of MAX_LOCAL + 8
+// frames never fills here and no root is abandoned; where the reference's
+// stack does not fill, the two enumerate the same sets.
+static const int MAX_DEPTH = MAX_LOCAL + 8;
 
 struct Params { int k, q, truss; };
 
@@ -631,17 +637,15 @@ static void ksearch(const Sub& s, const Params& P, Stats& st, uint64_t& tasks, S
     };
     int sz = 0;
     res[0] = k - 1; br[0] = 1; state[0] = 0; sz = 1;
-    int depth_off = 0;
     if (job_d >= 0) {
         // job d of the root (see ks_start in the device code): the exclude-chain frame at
         // depth d, from state 2 (d < |C2|) or the chain's bottom leaf (d == |C2|)
         const int m = n - hop;
         for (int i = 0; i < job_d; ++i) { excl.push_back(cand2.back()); cand2.pop_back(); }
         state[0] = job_d < m ? 2 : 0;
-        depth_off = job_d;
     }
     while (sz) {
-        if (sz + depth_off >= MAX_DEPTH) { st.depth_cap++; break; }
+        if (sz >= MAX_DEPTH) { st.depth_cap++; break; }   // cannot happen (see MAX_DEPTH)
         const int f = sz - 1;
         const int tag = f + 1;
         switch (state[f]) {
@@ -971,10 +975,11 @@ long long oracle_preprocess(const uint32_t* off, const uint32_t* adj, uint32_t n
 
 #ifdef ORACLE_MAIN
 int main(int argc, char** argv) {
-    if (argc < 2) { fprintf(stderr, "usage: %s <graph.bin> -k K -q Q [-tr 0|1] [-threads N] [-roots B E]\n", argv[0]); return 1; }
+    if (argc < 2) { fprintf(stderr, "usage: %s <graph.bin> -k K -q Q [-tr 0|1] [-threads N] [-roots B E] [-shard I S] [-seq]\n", argv[0]); return 1; }
     int k = 2, q = 8, tr = 0, th = 0;
     bool seq = false;
     uint64_t rb = 0, re = UINT64_MAX;
+    uint32_t si = 0, sc = 1;
     for (int i = 2; i < argc; ++i) {
         if (!strcmp(argv[i], "-k") && i + 1 < argc) k = atoi(argv[++i]);
         else if (!strcmp(argv[i], "-q") && i + 1 < argc) q = atoi(argv[++i]);
@@ -982,11 +987,12 @@ int main(int argc, char** argv) {
         else if (!strcmp(argv[i], "-threads") && i + 1 < argc) th = atoi(argv[++i]);
         else if (!strcmp(argv[i], "-roots") && i + 2 < argc) { rb = strtoull(argv[++i], 0, 10); re = strtoull(argv[++i], 0, 10); }
         else if (!strcmp(argv[i], "-seq")) seq = true;
+        else if (!strcmp(argv[i], "-shard") && i + 2 < argc) { si = (uint32_t)atoi(argv[++i]); sc = (uint32_t)atoi(argv[++i]); }
     }
     oracle::Graph g;
     if (oracle::load_bin(argv[1], g)) { fprintf(stderr, "cannot read %s\n", argv[1]); return 2; }
     oracle::Params P{k, q, tr};
-    oracle::Result R = oracle::run(g, P, th, rb, re, 0, 1, seq);
+    oracle::Result R = oracle::run(g, P, th, rb, re, si, sc, seq);
     printf("pn=%u pm=%u valid_roots=%llu max_n=%u max_left=%u truncated=%llu depth_capped=%llu oversized=%llu\n",
            R.pn, R.pm, (unsigned long long)R.valid, R.max_n, R.max_left, (unsigned long long)R.truncated,
            (unsigned long long)R.depth_cap, (unsigned long long)R.too_big);
