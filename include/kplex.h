@@ -59,6 +59,9 @@ typedef struct {
     uint32_t blocks_per_sm; /* persistent search kernel: 8-warp blocks per SM, 2 or 3 (0 = 2) */
     int32_t stage_after;    /* branch nodes a warp processes on one root before it copies the root's
                                adjacency matrix to shared memory (0 = 8, < 0 = never) */
+    uint32_t root_begin;    /* search only the roots of degeneracy rank r in [root_begin, root_end) */
+    uint32_t root_end;      /* (0/0 = all; combined with the shard rule above; a bounded, stated
+                               subset of a graph too large to enumerate whole) */
 } kplex_params;
 
 /* Results.  count/hash are the parity outputs; the rest mirrors the

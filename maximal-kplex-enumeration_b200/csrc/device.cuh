@@ -152,6 +152,7 @@ struct SearchParams {
     uint32_t low_water;        // a branch warp donates work when the pool holds fewer records
     uint32_t hash_on;
     uint32_t shard_index, shard_count;
+    uint32_t root_begin, root_end;   // roots of rank r outside [root_begin, root_end) are skipped
     uint32_t test_stuck;       // test hook: the first push claims a slot and never publishes it
     const GraphInfo* graphs;   // ngraphs entries
     uint32_t ngraphs;

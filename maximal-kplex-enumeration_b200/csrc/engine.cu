@@ -258,7 +258,8 @@ static int prepare_impl(const uint32_t* off, const uint32_t* adj, uint32_t n, ui
 static bool same_params(const kplex_params& a, const kplex_params& b) {
     return a.k == b.k && a.q == b.q && a.thres == b.thres && a.truss == b.truss && a.flags == b.flags &&
            a.device == b.device && a.pool_slots == b.pool_slots && a.shard_index == b.shard_index &&
-           a.shard_count == b.shard_count && a.blocks_per_sm == b.blocks_per_sm && a.stage_after == b.stage_after;
+           a.shard_count == b.shard_count && a.blocks_per_sm == b.blocks_per_sm && a.stage_after == b.stage_after &&
+           a.root_begin == b.root_begin && a.root_end == b.root_end;
 }
 
 static void fill_result(const kplex_prepared* h, const Counters& hc, float ms, double ms_dec, double ms_bnb,
@@ -423,6 +424,8 @@ int search_impl(kplex_prepared* h, Workspace* d, kplex_result* out, kplex_result
     sp.hash_on = (P.flags & KPLEX_FLAG_NO_HASH) ? 0u : 1u;
     sp.shard_index = P.shard_count > 1 ? P.shard_index : 0u;
     sp.shard_count = P.shard_count > 1 ? P.shard_count : 1u;
+    sp.root_begin = P.root_end ? P.root_begin : 0u;
+    sp.root_end = P.root_end ? P.root_end : 0xffffffffu;
     sp.spin_limit = 1ull << 24;
 
     if ((rc = d->ctr.ensure(sizeof(Counters)))) return rc;
@@ -461,6 +464,11 @@ int search_impl(kplex_prepared* h, Workspace* d, kplex_result* out, kplex_result
     if (hc.error) {
         g_last_error = hc.error == KPLEX_ERR_CAPACITY ? "a root's 2-hop subgraph exceeds 2048 vertices or its left set 8192"
                                                       : "device error in decomposition";
+        if (out) {   // the sizes that failed, for the caller's message
+            out->max_local_n = hc.max_n;
+            out->max_left = hc.max_left;
+            out->valid_roots = hc.valid_roots;
+        }
         return (int)hc.error;
     }
     // k-search jobs: a valid root with |C2| = n - hop owns |C2| + 1 independent jobs

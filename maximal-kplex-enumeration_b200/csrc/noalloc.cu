@@ -144,6 +144,8 @@ extern "C" int kplex_search_noalloc(const uint32_t* d_off, const uint32_t* d_adj
     sp.hash_on = (p->flags & KPLEX_FLAG_NO_HASH) ? 0u : 1u;
     sp.shard_index = p->shard_count > 1 ? p->shard_index : 0u;
     sp.shard_count = p->shard_count > 1 ? p->shard_count : 1u;
+    sp.root_begin = p->root_end ? p->root_begin : 0u;
+    sp.root_end = p->root_end ? p->root_end : 0xffffffffu;
     sp.spin_limit = 1ull << 24;
     uint32_t launches = 0;
 

@@ -32,7 +32,8 @@ class Params(ctypes.Structure):
     _fields_ = [("k", ctypes.c_int), ("q", ctypes.c_int), ("thres", ctypes.c_float), ("truss", ctypes.c_int),
                 ("flags", ctypes.c_uint32), ("device", ctypes.c_int), ("pool_slots", ctypes.c_uint64),
                 ("omp_threads", ctypes.c_uint32), ("shard_index", ctypes.c_uint32), ("shard_count", ctypes.c_uint32),
-                ("blocks_per_sm", ctypes.c_uint32), ("stage_after", ctypes.c_int32)]
+                ("blocks_per_sm", ctypes.c_uint32), ("stage_after", ctypes.c_int32), ("root_begin", ctypes.c_uint32),
+                ("root_end", ctypes.c_uint32)]
 
 
 class Result(ctypes.Structure):
@@ -209,17 +210,21 @@ def workload_graph(name: str):
 
 def make_params(k: int, q: int, thres: float = 0.25, truss: int = 0, flags: int = FLAG_QUIET, device: int = 0,
                 pool_slots: int = 0, omp_threads: int = 0, shard_index: int = 0, shard_count: int = 0,
-                blocks_per_sm: int = 0, stage_after: int = 0) -> Params:
+                blocks_per_sm: int = 0, stage_after: int = 0, root_begin: int = 0, root_end: int = 0) -> Params:
     return Params(k, q, thres, truss, flags, device, pool_slots, omp_threads, shard_index, shard_count,
-                  blocks_per_sm, stage_after)
+                  blocks_per_sm, stage_after, root_begin, root_end)
 
 
 def enumerate_csr(off: np.ndarray, adj: np.ndarray, k: int, q: int, thres: float = 0.25, truss: int = 0,
                   flags: int = FLAG_QUIET, device: int = 0, pool_slots: int = 0, check: bool = True,
-                  shard_index: int = 0, shard_count: int = 0) -> dict:
+                  shard_index: int = 0, shard_count: int = 0, root_begin: int = 0, root_end: int = 0) -> dict:
+    """Count and hash of the maximal k-plexes with >= q vertices (kplex_enumerate_csr).
+    root_begin/root_end (end 0 = all) and shard_index/shard_count restrict the
+    search to a stated subset of roots by degeneracy rank."""
     off = np.ascontiguousarray(off, dtype=np.uint32)
     adj = np.ascontiguousarray(adj, dtype=np.uint32)
-    p = make_params(k, q, thres, truss, flags, device, pool_slots, 0, shard_index, shard_count)
+    p = make_params(k, q, thres, truss, flags, device, pool_slots, 0, shard_index, shard_count,
+                    root_begin=root_begin, root_end=root_end)
     r = Result()
     rc = lib().kplex_enumerate_csr(_u32p(off), _u32p(adj), len(off) - 1, len(adj), ctypes.byref(p), ctypes.byref(r))
     if rc and check:
@@ -258,10 +263,11 @@ class Prepared:
 
 def prepare(off: np.ndarray, adj: np.ndarray, k: int, q: int, thres: float = 0.25, truss: int = 0,
             flags: int = FLAG_QUIET, device: int = 0, pool_slots: int = 0, shard_index: int = 0,
-            shard_count: int = 0) -> Prepared:
+            shard_count: int = 0, root_begin: int = 0, root_end: int = 0) -> Prepared:
     off = np.ascontiguousarray(off, dtype=np.uint32)
     adj = np.ascontiguousarray(adj, dtype=np.uint32)
-    p = make_params(k, q, thres, truss, flags, device, pool_slots, 0, shard_index, shard_count)
+    p = make_params(k, q, thres, truss, flags, device, pool_slots, 0, shard_index, shard_count,
+                    root_begin=root_begin, root_end=root_end)
     h = ctypes.c_void_p()
     r = Result()
     rc = lib().kplex_prepare(_u32p(off), _u32p(adj), len(off) - 1, len(adj), ctypes.byref(p), ctypes.byref(h), ctypes.byref(r))

@@ -58,3 +58,31 @@ def test_no_silent_cpu_path_without_a_device(kp):
     with pytest.raises(kp.KplexError) as e:
         kp.Server(slots=1)
     assert e.value.status == kp.ERR_NO_DEVICE
+
+
+def test_struct_layouts_match_header(kp, tmp_path):
+    """The ctypes mirrors in kplex_b200.py have the sizes and field offsets the C
+    compiler gives the structs of include/kplex.h (a field added on one side only
+    would shift every later field)."""
+    import ctypes
+    structs = {"kplex_params": kp.Params, "kplex_result": kp.Result, "kplex_graph": kp.Graph, "kplex_job": kp.Job,
+               "kplex_gen_spec": kp.GenSpec, "kplex_server_config": kp.ServerConfig,
+               "kplex_completion": kp.Completion, "kplex_server_stats": kp.ServerStats}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "kplex.h"', "int main(void) {"]
+    for cname, py in structs.items():
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, _ in py._fields_:
+            lines.append(f'  printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines.append("  return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = {}
+    for line in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.splitlines():
+        cname, key, val = line.split()
+        got[(cname, key)] = int(val)
+    for cname, py in structs.items():
+        assert got[(cname, "size")] == ctypes.sizeof(py), cname
+        for fname, _ in py._fields_:
+            assert got[(cname, fname)] == getattr(py, fname).offset, (cname, fname)

@@ -59,6 +59,31 @@ def test_left_sets_beyond_1024(kp, orc):
     assert (g["count"], g["hash"], g["tasks"]) == (o["count"], o["hash"], o["tasks"])
 
 
+def test_big_root_analytic(kp, orc):
+    """Roots of 1,105 local vertices (two bitset words per lane): the count and
+    hash equal the ones derived by hand for this graph, and the task count the
+    oracle's."""
+    from conftest import big_root_expected, big_root_graph
+    off, adj = big_root_graph(1100)
+    g = kp.enumerate_csr(off, adj, 2, 6)
+    e = big_root_expected(1100)
+    assert g["max_local_n"] == 1105
+    assert (g["count"], g["hash"]) == (e["count"], e["hash"])
+    o = orc.enumerate_csr(off, adj, 2, 6, threads=4)
+    assert g["tasks"] == o["tasks"]
+
+
+@pytest.mark.parametrize("nbig,core,p,k,q", [(1150, 4, 0.003, 2, 6), (1200, 5, 0.004, 3, 9)])
+def test_big_root_random(kp, orc, nbig, core, p, k, q):
+    """Roots above 1024 local vertices with random structure among their C2."""
+    from conftest import big_root_graph
+    off, adj = big_root_graph(nbig, core, p, seed=5)
+    g = kp.enumerate_csr(off, adj, k, q)
+    o = orc.enumerate_csr(off, adj, k, q, threads=4)
+    assert g["max_local_n"] == o["max_n"] > 1024
+    assert (g["count"], g["hash"], g["tasks"], g["valid_roots"]) == (o["count"], o["hash"], o["tasks"], o["valid_roots"])
+
+
 def test_edge_cases(kp):
     # empty graph, no vertex survives the core, graph too small for any root
     off = np.zeros(1, np.uint32)

@@ -47,37 +47,15 @@ def test_bounded_wait_reports_timeout(kp, orc):
     assert ok["status"] == 0 and ok["count"] > 0
 
 
-def _oversized_graph():
-    """root 0 adjacent to 550 of a 600-clique A; 500 vertices B adjacent to all of A.
-    Root 0 is first in the degeneracy order; C1 = its 550 neighbours, C2 = the other
-    50 A-vertices and all of B (550 common neighbours each) -> 1 + 550 + 550 > 1024."""
-    A = list(range(1, 601))
-    B = list(range(601, 1101))
-    adj = {v: set() for v in range(1101)}
-    def add(a, b):
-        adj[a].add(b); adj[b].add(a)
-    for i in A[:550]:
-        add(0, i)
-    for x in range(len(A)):
-        for y in range(x + 1, len(A)):
-            add(A[x], A[y])
-    for b in B:
-        for a in A:
-            add(a, b)
-    n = 1101
-    off = np.zeros(n + 1, np.uint32)
-    off[1:] = np.cumsum([len(adj[v]) for v in range(n)])
-    flat = np.concatenate([np.array(sorted(adj[v]), np.uint32) for v in range(n)])
-    return off, flat
-
-
 def test_oversized_root_is_an_error(kp):
-    """A root whose 2-hop subgraph exceeds 1024 vertices is beyond the reference's
-    MAX_BLK_SIZE (inc/common.h:8): the reference's 2-hop append (src/device_funcs.cu:255)
-    overruns its buffer there; this returns a status and the device stays usable."""
-    off, adj = _oversized_graph()
+    """A root whose 2-hop subgraph exceeds MAX_LOCAL = 2048 vertices returns
+    KPLEX_ERR_CAPACITY (the reference overruns its 1024-entry buffer there,
+    src/device_funcs.cu:255), and the device stays usable."""
+    from conftest import oversized_root_graph
+    off, adj = oversized_root_graph(1100, 1000, 1000)
     g = kp.enumerate_csr(off, adj, 2, 20, check=False)
     assert g["status"] == kp.ERR_CAPACITY
+    assert g["max_local_n"] > 2048
     small = kp.workload_graph("small")
     assert kp.enumerate_csr(*small, 2, 8)["count"] > 0
 

@@ -99,3 +99,17 @@ def test_oracle_left_sets_beyond_1024(orc):
     assert a["max_left"] > 1024 and a["oversized_roots"] == 0
     assert (a["count"], a["hash"]) == (b["count"], b["hash"])
     assert a["count"] == 629841
+
+
+def test_big_root_oracle_matches_hand_count(orc):
+    """The oracle on roots above 1024 local vertices (big_root_graph): the hand-derived
+    count and hash, and brute force on a small member of the same family."""
+    from conftest import big_root_expected, big_root_graph
+    off, adj = big_root_graph(1100)
+    o = orc.enumerate_csr(off, adj, 2, 6, threads=4)
+    e = big_root_expected(1100)
+    assert o["max_n"] == 1105
+    assert (o["count"], o["hash"]) == (e["count"], e["hash"])
+    off, adj = big_root_graph(40)
+    b = orc.bruteforce_csr(off, adj, 2, 6)
+    assert (b["count"], b["hash"]) == (big_root_expected(40)["count"], big_root_expected(40)["hash"])
