@@ -183,3 +183,24 @@ def big_root_expected(nbig=1100):
     pairs = np.column_stack([np.tile(np.arange(4, dtype=np.uint64), (len(iv), 1)), S[iv], S[iw]])
     h = (plex_hash_sum(with_r) + plex_hash_sum(pairs)) % (1 << 64)
     return {"count": nbig + nbig * (nbig - 1) // 2, "hash": h}
+
+
+def dense_request_graph():
+    """1,101 vertices, about 480,000 edges: root 0 adjacent to 550 of a 600-clique A,
+    and 500 vertices B adjacent to all of A.  Root 0's local subgraph has
+    1 + 550 + 550 vertices; a request whose device estimate is far above the
+    small batched graphs'."""
+    import numpy as np
+    A = np.arange(1, 601)
+    B = np.arange(601, 1101)
+    n = 1101
+    ia, ib = np.triu_indices(600, 1)
+    s = np.concatenate([np.zeros(550, np.int64), A[ia], np.repeat(A, 500)])
+    d = np.concatenate([A[:550], A[ib], np.tile(B, 600)])
+    u = np.concatenate([s, d])
+    v = np.concatenate([d, s])
+    order = np.lexsort((v, u))
+    u, v = u[order], v[order]
+    off = np.zeros(n + 1, np.uint32)
+    off[1:] = np.cumsum(np.bincount(u, minlength=n))
+    return off, v.astype(np.uint32)

@@ -9,7 +9,7 @@ import time
 import numpy as np
 import pytest
 
-from test_gpu_scheduling import _oversized_graph
+from conftest import dense_request_graph, oversized_root_graph
 
 pytestmark = pytest.mark.gpu
 
@@ -23,7 +23,7 @@ def _collect(srv, n, timeout_s=300):
     return got
 
 
-def test_server_results_match_plain_calls(kp):
+def test_server_results_match_plain_calls(kp, orc):
     graphs = kp.batch_workload(count=40, seed=11)
     small = kp.workload_graph("small")
     graphs.append((small[0], small[1], 2, 8))
@@ -40,6 +40,9 @@ def test_server_results_match_plain_calls(kp):
         assert c["status"] == 0
         assert (c["count"], c["hash"], c["valid_roots"]) == (one["count"], one["hash"], one["valid_roots"]), i
         assert c["ms_latency"] >= c["ms_service"] > 0
+        if i % 8 == 0:   # and a sample against the oracle, not only against the device
+            o = orc.enumerate_csr(off, adj, k, q, threads=4)
+            assert (c["count"], c["hash"], c["valid_roots"]) == (o["count"], o["hash"], o["valid_roots"]), i
     assert got[len(graphs) - 1]["count"] == 871
 
 
@@ -59,7 +62,7 @@ def test_server_split_grid_overlaps(kp):
 
 def test_server_memory_admission(kp):
     graphs = kp.batch_workload(count=6, seed=13)
-    big = _oversized_graph()
+    big = dense_request_graph()
     # a budget that holds the largest request's estimate (about 1.75 MB) but not two of
     # them, and no workspace: each request is admitted only when nothing else is in flight
     with kp.Server(slots=2, max_batch=8, mem_budget=1_800_000) as srv:
@@ -78,7 +81,7 @@ def test_server_memory_admission(kp):
 
 
 def test_server_isolates_failing_request(kp):
-    bad = _oversized_graph()
+    bad = oversized_root_graph(1100, 1000, 1000)
     graphs = kp.batch_workload(count=5, seed=14)
     with kp.Server(slots=1, max_batch=16) as srv:
         with pytest.raises(kp.KplexError):
@@ -92,3 +95,25 @@ def test_server_isolates_failing_request(kp):
     for i, (off, adj, k, q) in enumerate(graphs):
         one = kp.enumerate_csr(off, adj, k, q)
         assert got[i]["status"] == 0 and (got[i]["count"], got[i]["hash"]) == (one["count"], one["hash"])
+
+
+def test_server_large_request_runs_alone(kp):
+    """A request whose device estimate reaches large_bytes gets a launch of its own:
+    with large_bytes = 1 every request is large and runs alone; with the rule off
+    (UINT64_MAX) the same queue is batched."""
+    graphs = kp.batch_workload(count=8, seed=15)
+    for large, want_alone in ((1, True), (2**64 - 1, False)):
+        with kp.Server(slots=1, max_batch=16, large_bytes=large) as srv:
+            for i, (off, adj, k, q) in enumerate(graphs):
+                srv.submit(off, adj, k, q, tag=i)
+            srv.drain(timeout_ms=300_000)
+            got = {c["tag"]: c for c in srv.poll(64)}
+            st = srv.stats()
+        assert len(got) == len(graphs)
+        if want_alone:
+            assert all(c["batch_size"] == 1 for c in got.values()) and st["max_batch_seen"] == 1
+        else:
+            assert st["max_batch_seen"] >= 2
+        for i, (off, adj, k, q) in enumerate(graphs):
+            ref = kp.enumerate_csr(off, adj, k, q)
+            assert got[i]["status"] == 0 and (got[i]["count"], got[i]["hash"]) == (ref["count"], ref["hash"])
