@@ -39,7 +39,20 @@ DEFAULT_WORKLOAD = os.path.join(ROOT, "datasets", "soc-epinions.bin") + ":4:30:0
 UNIT = "plexes/s"
 
 
-def load_workload(name: str):
+def read_bin(path: str):
+    """The reference's .bin layout (inc/graph.h:45-62): u32 n, u32 m, u32 degree[n],
+    then the neighbour lists.  Read with numpy so that the reference arm loads no
+    library of this repository."""
+    raw = np.fromfile(path, dtype=np.uint32)
+    n, m = int(raw[0]), int(raw[1])
+    if raw.size != 2 + n + m:
+        raise ValueError(f"{path}: size does not match its header")
+    off = np.zeros(n + 1, np.uint32)
+    off[1:] = np.cumsum(raw[2:2 + n], dtype=np.uint64).astype(np.uint32)
+    return off, raw[2 + n:].copy()
+
+
+def load_workload(name: str, numpy_reader: bool = False):
     if name in kp.WORKLOADS:
         w = kp.WORKLOADS[name]
         off, adj = kp.workload_graph(name)
@@ -53,10 +66,10 @@ def load_workload(name: str):
                               m_directed=int(len(adj)), k=k, q=q, t=0.25, truss=0)
     # a real .bin graph: name = path:k:q:truss
     path, k, q, tr = name.split(":")
-    off, adj = kp.load_bin(path)
+    off, adj = read_bin(path) if numpy_reader else kp.load_bin(path)
     return off, adj, dict(workload=os.path.basename(path) + f" k={k} q={q} truss={tr}", n=int(len(off) - 1),
                           m_directed=int(len(adj)),
-                          k=int(k), q=int(q), t=0.25, truss=int(tr))
+                          k=int(k), q=int(q), t=0.25, truss=int(tr), input=os.path.relpath(path, ROOT))
 
 
 def data_kind(cfg) -> str:
@@ -139,29 +152,62 @@ def allreduce_results(dist, count: int, hsum: int, ms: float, device) -> tuple[i
     return int(tot[0].item()), int(tot[1].item()) & ((1 << 64) - 1), float(mx.item())
 
 
-def cpu_sample(off, adj, cfg, budget_s: float = 20.0, span: int | None = None):
-    """Oracle (OpenMP, all host cores) on a bounded root sample of the workload: the
-    latest-ranked roots (where nearly all plexes of a degeneracy order lie), a range
-    grown 2x at a time from 1/1024 of the roots until one run takes budget_s / 4, or
-    exactly `span` roots when given.  Returns the baseline dict and the span used."""
+def cpu_sample(off, adj, cfg, budget_s: float = 20.0, stride: int | None = None):
+    """Oracle (OpenMP, all host cores) on a stratified root sample of the workload:
+    the roots whose degeneracy rank r has r % stride == 0, spread over the whole
+    order so that the sample's plexes per second stand for the whole graph's.  The
+    stride starts near nroots / 8 and halves (doubling the sample) until one run
+    takes budget_s / 4, or is `stride` when given.  Returns the baseline dict and
+    the stride used."""
     sys.path.insert(0, ROOT)
     import oracle  # CPU baseline only
 
     pre = oracle.preprocess(off, adj, cfg["k"], cfg["q"], cfg["truss"])
-    nroots = max(0, pre["pn"] - cfg["q"] + 2)
-    fixed = span is not None
-    span = max(1, span if fixed else nroots // 1024)
+    nroots = max(1, pre["pn"] - cfg["q"] + 2)
+    fixed = stride is not None
+    if not fixed:
+        stride = 1
+        while stride * 16 <= nroots:
+            stride *= 2
     while True:
-        b = max(0, nroots - span)
         t0 = time.perf_counter()
-        r = oracle.enumerate_csr(off, adj, cfg["k"], cfg["q"], cfg["truss"], threads=0, root_begin=b, root_end=nroots)
+        r = oracle.enumerate_shard(off, adj, cfg["k"], cfg["q"], cfg["truss"], 0, stride, threads=0)
         el = time.perf_counter() - t0
-        if fixed or el >= budget_s / 4 or span >= nroots:
+        if fixed or el >= budget_s / 4 or stride == 1:
             break
-        span = min(nroots, span * 2)
+        stride //= 2
+    nsample = (nroots + stride - 1) // stride
     return {"value": r["count"] / el if el > 0 else 0.0, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
-            "sample": f"roots of degeneracy rank [{b},{nroots}) of {nroots}: {r['count']} plexes in {el:.2f} s "
-                      f"(oracle restatement, all {os.cpu_count()} host threads)"}, span
+            "sample": f"roots of degeneracy rank r % {stride} == 0 ({nsample} of {nroots}, spread over the whole "
+                      f"order): {r['count']} plexes in {el:.2f} s (oracle restatement, preprocessing included, "
+                      f"all {os.cpu_count()} host threads)"}, stride
+
+
+def cudaplex_run(cfg, timeout_s: float = 300.0):
+    """The reference CudaPlex, unmodified and rebuilt for sm_100a (oracle/_ref/cudaplex,
+    compile.sh:5 with -arch changed), run once on this GPU on the same graph and
+    parameters, outside the timed steps.  Returns its own "Total Time Elapsed"
+    (preprocessing + search, inc/host_funcs.h:747-858, 1021-1149), its count and the
+    process wall time, or None when the binary or the .bin input is absent."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "cudaplex")
+    path = os.path.join(ROOT, cfg["input"]) if cfg.get("input") else None
+    if not path or not os.path.exists(exe) or not os.path.exists(path):
+        return None
+    cmd = [exe, path, "-k", str(cfg["k"]), "-q", str(cfg["q"]), "-t", str(cfg["t"]), "-tr", str(cfg["truss"])]
+    t0 = time.perf_counter()
+    try:
+        out = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout_s).stdout
+    except (subprocess.TimeoutExpired, OSError) as e:
+        return {"error": str(e)[:200]}
+    wall = (time.perf_counter() - t0) * 1e3
+    rec = {"command": " ".join(["oracle/_ref/cudaplex", os.path.relpath(path, ROOT)] + cmd[2:]), "wall_ms": wall}
+    for line in out.splitlines():
+        if line.startswith("Total Time Elapsed:"):
+            rec["ms_ref_region"] = float(line.split(":")[1].split()[0])
+        elif "Maximal k-Plexes:" in line:
+            rec["count"] = int(line.rsplit(":", 1)[1])
+            rec["valid_blocks"] = int(line.split("Total Valid Blocks:")[1].split(",")[0])
+    return rec
 
 
 def run_reference(args, cfg, off, adj):
@@ -169,9 +215,9 @@ def run_reference(args, cfg, off, adj):
     if rank != 0:
         return
     steps = []
-    span = None   # sized on the first (warm-up) step, then fixed
+    stride = None   # sized on the first (warm-up) step, then fixed
     for i in range(args.warmup + args.steps):
-        cb, span = cpu_sample(off, adj, cfg, budget_s=args.cpu_budget, span=span)
+        cb, stride = cpu_sample(off, adj, cfg, budget_s=args.cpu_budget, stride=stride)
         if i >= args.warmup:
             steps.append(cb)
     v = statistics.median([s["value"] for s in steps])
@@ -350,6 +396,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cudaplex", action="store_true",
+                    help="skip the one run of the reference CudaPlex (oracle/_ref/cudaplex) on the same graph")
     ap.add_argument("--mode", default="plain", choices=["plain", "batched", "served"],
                     help="plain: one graph per step (the headline); batched: many graphs per launch; "
                          "served: an open-loop request stream through the server")
@@ -375,7 +423,7 @@ def main():
     if args.workload is None:
         args.workload = DEFAULT_WORKLOAD if os.path.exists(DEFAULT_WORKLOAD.split(":")[0]) else "small"
 
-    off, adj, cfg = load_workload(args.workload)
+    off, adj, cfg = load_workload(args.workload, numpy_reader=args.impl == "reference")
     if args.impl == "reference":
         run_reference(args, cfg, off, adj)
         return
@@ -434,14 +482,17 @@ def main():
 
     # end to end through the public C ABI from host CSR arrays (rank's shard)
     e2e_ms = []
+    e2e_ref = []
     e2e_count = 0
     e2e_parts = {}
     for _ in range(args.e2e_steps):
         r = kp.enumerate_csr(off, adj, cfg["k"], cfg["q"], cfg["t"], cfg["truss"], device=local,
                              shard_index=shard_index, shard_count=shard_count)
         e2e_ms.append(r["ms_total"])
+        e2e_ref.append(r["ms_ref_region"])
         e2e_count = r["count"]
-        e2e_parts = {"ms_preprocess": r["ms_preprocess"], "ms_device": r["ms_device"], "ms_total": r["ms_total"]}
+        e2e_parts = {"ms_preprocess": r["ms_preprocess"], "ms_device": r["ms_device"],
+                     "ms_ref_region": r["ms_ref_region"], "ms_total": r["ms_total"]}
     if world > 1:
         e = torch.tensor([max(e2e_ms)], dtype=torch.float64, device=f"cuda:{local}")
         dist.all_reduce(e, op=dist.ReduceOp.MAX)
@@ -495,6 +546,17 @@ def main():
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_sample(off, adj, cfg, budget_s=args.cpu_budget)[0]
+    if rank == 0 and world == 1 and not args.no_cudaplex and shard_count == 0:
+        ref = cudaplex_run(cfg)
+        if ref is not None:
+            line["cudaplex_sm100a"] = ref
+            if "ms_ref_region" in ref and e2e_ref:
+                ours_ref = statistics.median(e2e_ref)
+                # the same boundary on both sides: preprocessing + device search
+                line["vs_cudaplex"] = {"ref_region": ref["ms_ref_region"] / ours_ref,
+                                       "wall": ref["wall_ms"] / e2e_max if e2e_max > 0 else None,
+                                       "ours_ms_ref_region": ours_ref,
+                                       "count_equal": ref.get("count") == (total_count & 0xffffffff)}
     if rank == 0:
         print(json.dumps(line), flush=True)
     prep.release()
