@@ -411,6 +411,10 @@ def main():
     ap.add_argument("--no-split-grid", dest="split_grid", action="store_false",
                     help="served: give each launch the whole device instead of 1/slots of the SMs")
     ap.add_argument("--mem-budget", type=int, default=32, help="served: GiB")
+    ap.add_argument("--blocks-per-sm", type=int, default=0,
+                    help="plain: 8-warp blocks per SM of the search kernel (2 or 3; 0 = the library default)")
+    ap.add_argument("--stage-after", type=int, default=0,
+                    help="plain: branch nodes on one root before its adjacency matrix is staged in shared memory")
     ap.add_argument("--shards", type=int, default=1,
                     help="plain, one GPU: search only the roots of rank r % shards == 0 (a small case for profiling)")
     args = ap.parse_args()
@@ -450,8 +454,11 @@ def main():
     shard_index, shard_count = (rank, world) if world > 1 else (0, args.shards if args.shards > 1 else 0)
     if shard_count and world == 1:
         cfg["shard"] = f"roots r % {shard_count} == 0 only"
+    sched = dict(blocks_per_sm=args.blocks_per_sm, stage_after=args.stage_after)
+    if args.blocks_per_sm or args.stage_after:
+        cfg["schedule"] = {k: v for k, v in sched.items() if v}
     prep = kp.prepare(off, adj, cfg["k"], cfg["q"], cfg["t"], cfg["truss"], device=local,
-                      shard_index=shard_index, shard_count=shard_count)
+                      shard_index=shard_index, shard_count=shard_count, **sched)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
     for _ in range(args.warmup):
         prep.search()
@@ -487,7 +494,7 @@ def main():
     e2e_parts = {}
     for _ in range(args.e2e_steps):
         r = kp.enumerate_csr(off, adj, cfg["k"], cfg["q"], cfg["t"], cfg["truss"], device=local,
-                             shard_index=shard_index, shard_count=shard_count)
+                             shard_index=shard_index, shard_count=shard_count, **sched)
         e2e_ms.append(r["ms_total"])
         e2e_ref.append(r["ms_ref_region"])
         e2e_count = r["count"]

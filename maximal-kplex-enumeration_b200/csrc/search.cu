@@ -32,16 +32,19 @@
 namespace kplex {
 
 // ============================================================== root view
+// The root's block in the arena: A, M2, M4 ([n][W] each), LA ([n][WL]),
+// LT ([nleft][W]), sorig, srank ([n]).  Only A's address is kept; the others
+// are derived on use, which keeps a warp's registers for its search state.
 struct RootView {
     uint32_t n, hop, nleft, W, WL, graph;
     int k, q;
     const uint32_t* A;
-    const uint32_t* M2;
-    const uint32_t* M4;
-    const uint32_t* LA;
-    const uint32_t* LT;
-    const uint32_t* sorig;
-    const uint32_t* srank;
+    __device__ __forceinline__ const uint32_t* M2() const { return A + (uint64_t)n * W; }
+    __device__ __forceinline__ const uint32_t* M4() const { return A + 2ull * n * W; }
+    __device__ __forceinline__ const uint32_t* LA() const { return A + 3ull * n * W; }
+    __device__ __forceinline__ const uint32_t* LT() const { return LA() + (uint64_t)n * WL; }
+    __device__ __forceinline__ const uint32_t* sorig() const { return LT() + (uint64_t)nleft * W; }
+    __device__ __forceinline__ const uint32_t* srank() const { return sorig() + n; }
 };
 
 __device__ __forceinline__ RootView root_view(const SearchParams& sp, uint32_t r) {
@@ -49,14 +52,7 @@ __device__ __forceinline__ RootView root_view(const SearchParams& sp, uint32_t r
     RootView v;
     v.n = d.n; v.hop = d.hop; v.nleft = d.nleft; v.W = d.W; v.WL = d.WL;
     v.graph = d.graph; v.k = d.k; v.q = d.q;
-    const uint32_t* A = sp.arena + d.base;
-    v.A = A;
-    v.M2 = A + (uint64_t)d.n * d.W;
-    v.M4 = v.M2 + (uint64_t)d.n * d.W;
-    v.LA = v.M4 + (uint64_t)d.n * d.W;
-    v.LT = v.LA + (uint64_t)d.n * d.WL;
-    v.sorig = v.LT + (uint64_t)d.nleft * d.W;
-    v.srank = v.sorig + d.n;
+    v.A = sp.arena + d.base;
     return v;
 }
 
@@ -291,14 +287,14 @@ __device__ int ks_advance(const SearchParams& sp, const KsSlot<NW>& S, Emitted<N
 #pragma unroll
         for (int j = 0; j < NW; ++j) {
             const uint32_t wi = l + 32u * j;
-            const uint32_t m2 = (wi < W) ? __ldg(R.M2 + (uint64_t)node * W + wi) : 0u;
+            const uint32_t m2 = (wi < W) ? __ldg(R.M2() + (uint64_t)node * W + wi) : 0u;
             uint32_t drop = C1.w[j] & ~m2;
             C1.w[j] &= m2;
             while (drop) { const int b = __ffs(drop) - 1; S.t1()[wi * 32 + b] = tag; drop &= drop - 1; }
         }
     };
     auto update23 = [&](uint32_t node, uint16_t tag) {   // updateCand23, src:1099-1122 (order preserving)
-        const uint32_t* m2row = R.M2 + (uint64_t)node * W;
+        const uint32_t* m2row = R.M2() + (uint64_t)node * W;
         uint32_t write = 0;
         for (uint32_t b = 0; b < nc2; b += 32) {
             const uint32_t i = b + l;
@@ -507,27 +503,6 @@ __device__ __forceinline__ void rowg_popc2(const uint32_t* row, const uint32_t* 
     c2 = a2;
 }
 
-// Per-warp shared memory of the branch-and-bound, bitsets of BW = 32 * NW words.
-struct BnbSmem {
-    uint32_t* rec;    // slot_words: record being loaded from the pool
-    uint32_t* P;      // BW words each
-    uint32_t* PC;
-    uint32_t* SAT;
-    uint32_t* ROW;
-    uint32_t* M2;
-    uint32_t* M4;
-    uint32_t* NC;
-    uint32_t* NX;
-    uint32_t* SB;
-    uint16_t* list;   // nmax
-    uint16_t* gv;     // nmax
-    uint16_t* pv;     // nmax
-    unsigned long long* CT;   // 16 per-warp counters (lane 0 updates them; kept out of registers)
-    uint32_t* SCT;    // STACK_CACHE tags: the stack index each cached record was pushed at
-    uint32_t* SC;     // STACK_CACHE records of slot_words
-    uint32_t* A;      // a_words: the current root's adjacency matrix, when it fits
-};
-
 // The newest STACK_CACHE records a warp pushes on its depth-first stack are
 // also kept in its shared memory (tagged with their stack index), so that the
 // usual pop, of the record pushed last, does not wait for an L2 round trip.
@@ -545,27 +520,38 @@ __host__ __device__ inline uint32_t bnb_smem_words(uint32_t nmax, uint32_t slot_
     return bnb_fixed_words(nmax, slot_words, bw) + 32u + stack_cache_words(slot_words) + a_words;
 }
 
-__device__ inline BnbSmem bnb_smem(uint32_t* base, uint32_t nmax, uint32_t slot_words, uint32_t bw) {
-    BnbSmem m;
-    uint32_t* p = base;
-    m.rec = p; p += slot_words;
-    m.P = p; p += bw;
-    m.PC = p; p += bw;
-    m.SAT = p; p += bw;
-    m.ROW = p; p += bw;
-    m.M2 = p; p += bw;
-    m.M4 = p; p += bw;
-    m.NC = p; p += bw;
-    m.NX = p; p += bw;
-    m.SB = p; p += bw;
-    m.list = reinterpret_cast<uint16_t*>(p); p += (nmax + 1) / 2;
-    m.gv = reinterpret_cast<uint16_t*>(p); p += (nmax + 1) / 2;
-    m.pv = reinterpret_cast<uint16_t*>(p); p += (nmax + 1) / 2;
-    m.CT = reinterpret_cast<unsigned long long*>(base + bnb_fixed_words(nmax, slot_words, bw));
-    m.SCT = reinterpret_cast<uint32_t*>(m.CT + 16);
-    m.SC = m.SCT + STACK_CACHE;
-    m.A = m.SCT + stack_cache_words(slot_words);
-    return m;
+// Per-warp shared memory of the branch-and-bound.  In words from the warp's base:
+//   rec [slot_words] | P, PC, SAT, ROW, M2, M4, NC, NX, SB [BW each] |
+//   list, gv, pv [nmax u16 each] | 16 counters (u64) | STACK_CACHE tags + records | A [a_words]
+// with BW = 32 * NW.  Only the base address and two sizes are kept; every region's
+// address is derived on use, which keeps a warp's registers for its search state.
+struct BnbSmem {
+    uint32_t* base;
+    uint32_t sw;     // slot_words
+    uint32_t half;   // words of one u16 list of nmax entries
+    uint32_t bw;     // bitset words
+    __device__ __forceinline__ uint32_t* rec() const { return base; }
+    __device__ __forceinline__ uint32_t* P() const { return base + sw; }
+    __device__ __forceinline__ uint32_t* PC() const { return base + sw + bw; }
+    __device__ __forceinline__ uint32_t* SAT() const { return base + sw + 2 * bw; }
+    __device__ __forceinline__ uint32_t* ROW() const { return base + sw + 3 * bw; }
+    __device__ __forceinline__ uint32_t* M2() const { return base + sw + 4 * bw; }
+    __device__ __forceinline__ uint32_t* M4() const { return base + sw + 5 * bw; }
+    __device__ __forceinline__ uint32_t* NC() const { return base + sw + 6 * bw; }
+    __device__ __forceinline__ uint32_t* NX() const { return base + sw + 7 * bw; }
+    __device__ __forceinline__ uint32_t* SB() const { return base + sw + 8 * bw; }
+    __device__ __forceinline__ uint16_t* list() const { return reinterpret_cast<uint16_t*>(base + sw + 9 * bw); }
+    __device__ __forceinline__ uint16_t* gv() const { return reinterpret_cast<uint16_t*>(base + sw + 9 * bw + half); }
+    __device__ __forceinline__ uint16_t* pv() const { return reinterpret_cast<uint16_t*>(base + sw + 9 * bw + 2 * half); }
+    __device__ __forceinline__ uint32_t fixed() const { return (sw + 9 * bw + 3 * half + 3u) & ~3u; }
+    __device__ __forceinline__ unsigned long long* CT() const { return reinterpret_cast<unsigned long long*>(base + fixed()); }
+    __device__ __forceinline__ uint32_t* SCT() const { return base + fixed() + 32; }
+    __device__ __forceinline__ uint32_t* SC() const { return SCT() + STACK_CACHE; }
+    __device__ __forceinline__ uint32_t* A() const { return SCT() + stack_cache_words(sw); }
+};
+
+__device__ __forceinline__ BnbSmem bnb_smem(uint32_t* base, uint32_t nmax, uint32_t slot_words, uint32_t bw) {
+    return BnbSmem{base, slot_words, (nmax + 1) / 2, bw};
 }
 
 // The reference's warp pivot rule (src:1628-1663, 1669-1697): the shfl_down
@@ -612,14 +598,14 @@ __device__ bool left_maximal(const SearchParams& sp, const RootView& R, const Bn
             while (msk) {
                 const int j = __ffs(msk) - 1;
                 msk &= msk - 1;
-                const uint32_t u = m.list[b + j];
-                if (w < WL) lc &= __ldg(R.LA + (uint64_t)u * WL + w);
+                const uint32_t u = m.list()[b + j];
+                if (w < WL) lc &= __ldg(R.LA() + (uint64_t)u * WL + w);
             }
         }
         uint32_t un = 0;   // and to one of any k members
         for (int t = 0; t < k && t < s; ++t) {
-            const uint32_t u = m.list[t];
-            if (w < WL) un |= __ldg(R.LA + (uint64_t)u * WL + w);
+            const uint32_t u = m.list()[t];
+            if (w < WL) un |= __ldg(R.LA() + (uint64_t)u * WL + w);
         }
         lc &= un;
         bool f = false;
@@ -628,7 +614,7 @@ __device__ bool left_maximal(const SearchParams& sp, const RootView& R, const Bn
             const int bit = __ffs(c) - 1;
             c &= c - 1;
             const uint32_t j = w * 32 + bit;
-            const int cnt = row_and_popc(R.LT + (uint64_t)j * W, sS, W);
+            const int cnt = row_and_popc(R.LT() + (uint64_t)j * W, sS, W);
             ++nrows;
             if (cnt + k >= s + 1) f = true;
         }
@@ -646,11 +632,11 @@ __device__ void emit_plex(const SearchParams& sp, const RootView& R, const BnbSm
     const unsigned l = lane_id();
     if (l == 0) ++cnt;
     if (!sp.hash_on) return;
-    bits_fill<NW>(m.SB, 0u);
+    bits_fill<NW>(m.SB(), 0u);
     __syncwarp();
     for (int i = l; i < s; i += 32) {
-        const uint32_t rk = __ldg(R.srank + m.list[i]);
-        atomicOr(&m.SB[rk >> 5], 1u << (rk & 31));
+        const uint32_t rk = __ldg(R.srank() + m.list()[i]);
+        atomicOr(&m.SB()[rk >> 5], 1u << (rk & 31));
     }
     __syncwarp();
     // the sorted original ids, word by word in ascending order: lane L walks word
@@ -658,13 +644,13 @@ __device__ void emit_plex(const SearchParams& sp, const RootView& R, const BnbSm
     uint64_t x = plex_hash_begin((uint32_t)s);
 #pragma unroll
     for (int j = 0; j < NW; ++j) {
-        uint32_t w = m.SB[32 * j + l];
+        uint32_t w = m.SB()[32 * j + l];
         for (int L = 0; L < 32; ++L) {
             if ((int)l == L) {
                 while (w) {
                     const int b = __ffs(w) - 1;
                     w &= w - 1;
-                    x = plex_hash_step(x, __ldg(R.sorig + (32 * j + L) * 32 + b));
+                    x = plex_hash_step(x, __ldg(R.sorig() + (32 * j + L) * 32 + b));
                 }
             }
             x = __shfl_sync(FULL, x, L);
@@ -679,17 +665,20 @@ struct Node {
     Bits<NW> P, C, X;   // this lane's words of each bitset
 };
 
-// Counters live in the warp's shared memory (m.CT) and are updated by lane 0.
+// Counters live in the warp's shared memory (m.CT()) and are updated by lane 0.
 enum : int { CT_CNT, CT_HSUM, CT_TASKS, CT_NODES, CT_BB, CT_TOT_CNT, CT_TOT_HSUM, CT_STAGE, CT_KS_CYC, CT_SPILL,
              CT_REFILL, CT_BNB_CYC, CT_IDLE_CYC, CT_KS_TASKS };
+// A warp's depth-first stack (records [sbot, stop) of `stack`, a ring of
+// stack_depth records) and its counters in shared memory.
 struct WarpWork {
     uint32_t* stack;
     unsigned long long sbot, stop;
-    unsigned long long& cnt;
-    unsigned long long& hsum;
-    unsigned long long& tasks;
-    unsigned long long& nodes;
-    unsigned long long& bb;
+    unsigned long long* ct;
+    __device__ __forceinline__ unsigned long long& cnt() const { return ct[CT_CNT]; }
+    __device__ __forceinline__ unsigned long long& hsum() const { return ct[CT_HSUM]; }
+    __device__ __forceinline__ unsigned long long& tasks() const { return ct[CT_TASKS]; }
+    __device__ __forceinline__ unsigned long long& nodes() const { return ct[CT_NODES]; }
+    __device__ __forceinline__ unsigned long long& bb() const { return ct[CT_BB]; }
 };
 
 // One branch-and-bound node (BNB, src:1516-1724).  Returns true when the node
@@ -704,29 +693,29 @@ __device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootVie
     const uint32_t np = t->np, nc = t->nc, nx = t->nx;
     const Bits<NW> P = t->P, C = t->C, X = t->X;
     if ((int)(np + nc) < q) return false;
-    bits_store(m.P, P);
-    bits_store(m.PC, bits_or(P, C));
+    bits_store(m.P(), P);
+    bits_store(m.PC(), bits_or(P, C));
     __syncwarp();
-    bits_list(P, m.list);
-    bits_list(C, m.list + np);
+    bits_list(P, m.list());
+    bits_list(C, m.list() + np);
     const int tot = (int)(np + nc);
     for (int i = l; i < tot; i += 32) {
         int g, p;
-        rowg_popc2(A + (uint32_t)m.list[i] * W, m.PC, m.P, W, g, p);
-        m.gv[i] = (uint16_t)g;
-        m.pv[i] = (uint16_t)p;
+        rowg_popc2(A + (uint32_t)m.list()[i] * W, m.PC(), m.P(), W, g, p);
+        m.gv()[i] = (uint16_t)g;
+        m.pv()[i] = (uint16_t)p;
     }
-    if (l == 0) ww.bb += (unsigned long long)(tot + 3) * 4ull * W;   // rows + the record's P, C, X
+    if (l == 0) ww.bb() += (unsigned long long)(tot + 3) * 4ull * W;   // rows + the record's P, C, X
     __syncwarp();
     if (nc == 0) {   // src:1579-1588
-        if (nx == 0 && (int)np >= q && left_maximal(sp, R, m, (int)np, m.pv, m.P, ww.bb))
-            emit_plex<NW>(sp, R, m, (int)np, ww.cnt, ww.hsum);
+        if (nx == 0 && (int)np >= q && left_maximal(sp, R, m, (int)np, m.pv(), m.P(), ww.bb()))
+            emit_plex<NW>(sp, R, m, (int)np, ww.cnt(), ww.hsum());
         return false;
     }
     // pivot in P: minimum neiInG, ties to the smaller index (src:1592-1620)
     unsigned long long key = ~0ull;   // (neiInG, vertex, neiInP) of this lane's best P member
     for (int i = l; i < (int)np; i += 32) {
-        const unsigned long long kk = ((unsigned long long)m.gv[i] << 32) | ((unsigned long long)m.list[i] << 16) | m.pv[i];
+        const unsigned long long kk = ((unsigned long long)m.gv()[i] << 32) | ((unsigned long long)m.list()[i] << 16) | m.pv()[i];
         key = kk < key ? kk : key;
     }
     const unsigned kg = (unsigned)(key >> 32);
@@ -740,13 +729,13 @@ __device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootVie
     int piv, pmin, pval, pidx;
     if (minP + k < tot) {
         // candidates not adjacent to the P pivot (src:1626-1663)
-        bits_store(m.ROW, bits_load<NW>(A + (uint32_t)pp * W, W));
+        bits_store(m.ROW(), bits_load<NW>(A + (uint32_t)pp * W, W));
         __syncwarp();
         pmin = INT_MAX; piv = -1; pval = 0; pidx = -1;
         for (int i = l; i < (int)nc; i += 32) {
-            const uint32_t v = m.list[np + i];
-            if (test_bit(m.ROW, v)) continue;
-            const int g = m.gv[np + i], p = m.pv[np + i];
+            const uint32_t v = m.list()[np + i];
+            if (test_bit(m.ROW(), v)) continue;
+            const int g = m.gv()[np + i], p = m.pv()[np + i];
             if (g < pmin) { pmin = g; piv = (int)v; pval = p; pidx = (int)np + i; }
             else if (g == pmin && pval > p) { piv = (int)v; pval = p; pidx = (int)np + i; }
         }
@@ -755,8 +744,8 @@ __device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootVie
         // minimum over P (seeded) and C (src:1669-1697)
         pmin = minP; piv = pp; pval = ppP; pidx = -2;
         for (int i = l; i < (int)nc; i += 32) {
-            const uint32_t v = m.list[np + i];
-            const int g = m.gv[np + i], p = m.pv[np + i];
+            const uint32_t v = m.list()[np + i];
+            const int g = m.gv()[np + i], p = m.pv()[np + i];
             if (g < pmin) { pmin = g; piv = (int)v; pval = p; pidx = (int)np + i; }
             else if (g == pmin && pval > p) { piv = (int)v; pval = p; pidx = (int)np + i; }
         }
@@ -764,22 +753,22 @@ __device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootVie
         if (pmin >= tot - k) {
             // P ∪ C is a k-plex (src:1698-1717)
             if (tot < q) return false;
-            const int nxl = bits_list(X, m.list + tot);
+            const int nxl = bits_list(X, m.list() + tot);
             for (int i = l; i < nxl; i += 32)
-                m.gv[tot + i] = (uint16_t)rowg_popc(A + (uint32_t)m.list[tot + i] * W, m.PC, W);
-            bits_fill<NW>(m.SAT, 0u);
+                m.gv()[tot + i] = (uint16_t)rowg_popc(A + (uint32_t)m.list()[tot + i] * W, m.PC(), W);
+            bits_fill<NW>(m.SAT(), 0u);
             __syncwarp();
             for (int i = l; i < tot; i += 32)
-                if ((int)m.gv[i] + k == tot) { const uint32_t u = m.list[i]; atomicOr(&m.SAT[u >> 5], 1u << (u & 31)); }
+                if ((int)m.gv()[i] + k == tot) { const uint32_t u = m.list()[i]; atomicOr(&m.SAT()[u >> 5], 1u << (u & 31)); }
             __syncwarp();
             bool ext = false;
             for (int i = l; i < nxl; i += 32) {   // isKplexPC2 src:601-622
-                if ((int)m.gv[tot + i] + k < tot + 1) continue;
-                ext |= rowg_covers(A + (uint32_t)m.list[tot + i] * W, m.SAT, W);
+                if ((int)m.gv()[tot + i] + k < tot + 1) continue;
+                ext |= rowg_covers(A + (uint32_t)m.list()[tot + i] * W, m.SAT(), W);
             }
-            if (l == 0) ww.bb += (unsigned long long)nxl * 4ull * W;
+            if (l == 0) ww.bb() += (unsigned long long)nxl * 4ull * W;
             if (__any_sync(FULL, ext)) return false;
-            if (left_maximal(sp, R, m, tot, m.gv, m.PC, ww.bb)) emit_plex<NW>(sp, R, m, tot, ww.cnt, ww.hsum);
+            if (left_maximal(sp, R, m, tot, m.gv(), m.PC(), ww.bb())) emit_plex<NW>(sp, R, m, tot, ww.cnt(), ww.hsum());
             return false;
         }
     }
@@ -792,11 +781,11 @@ __device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootVie
         Bits<NW> Cx = C, Xx = X;
         bits_clear(Cx, v);
         bits_set(Xx, v);
-        uint32_t* cdst = m.SC + (uint32_t)(ww.stop % STACK_CACHE) * SW;   // shared-memory copy
+        uint32_t* cdst = m.SC() + (uint32_t)(ww.stop % STACK_CACHE) * SW;   // shared-memory copy
         if (l == 0) {
             __stcg(dst + 0, t->root); __stcg(dst + 1, np | ((nc - 1) << 16)); __stcg(dst + 2, nx + 1); __stcg(dst + 3, 0u);
             cdst[0] = t->root; cdst[1] = np | ((nc - 1) << 16); cdst[2] = nx + 1; cdst[3] = 0u;
-            m.SCT[ww.stop % STACK_CACHE] = (uint32_t)ww.stop;
+            m.SCT()[ww.stop % STACK_CACHE] = (uint32_t)ww.stop;
         }
 #pragma unroll
         for (int j = 0; j < NW; ++j) {
@@ -808,66 +797,66 @@ __device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootVie
         }
         __syncwarp();
         ++ww.stop;
-        if (l == 0) { ++ww.tasks; ww.bb += 12ull * W; }
+        if (l == 0) { ++ww.tasks(); ww.bb() += 12ull * W; }
     }
     // include child
     const uint32_t np1 = np + 1;
     Bits<NW> P1 = P;
     bits_set(P1, v);
-    bits_store(m.ROW, bits_load<NW>(A + v * W, W));
-    bits_store(m.M2, bits_ldg<NW>(R.M2 + (uint64_t)v * W, W));
-    bits_store(m.M4, bits_ldg<NW>(R.M4 + (uint64_t)v * W, W));
-    bits_fill<NW>(m.SAT, 0u);
-    bits_fill<NW>(m.NC, 0u);
-    bits_fill<NW>(m.NX, 0u);
+    bits_store(m.ROW(), bits_load<NW>(A + v * W, W));
+    bits_store(m.M2(), bits_ldg<NW>(R.M2() + (uint64_t)v * W, W));
+    bits_store(m.M4(), bits_ldg<NW>(R.M4() + (uint64_t)v * W, W));
+    bits_fill<NW>(m.SAT(), 0u);
+    bits_fill<NW>(m.NC(), 0u);
+    bits_fill<NW>(m.NX(), 0u);
     __syncwarp();
     // saturated members of P + v: neiInP' + k == |P'|
     for (int i = l; i < (int)np; i += 32) {
-        const uint32_t u = m.list[i];
-        const int pu = (int)m.pv[i] + (int)test_bit(m.ROW, u);
-        if (pu + k == (int)np1) atomicOr(&m.SAT[u >> 5], 1u << (u & 31));
+        const uint32_t u = m.list()[i];
+        const int pu = (int)m.pv()[i] + (int)test_bit(m.ROW(), u);
+        if (pu + k == (int)np1) atomicOr(&m.SAT()[u >> 5], 1u << (u & 31));
     }
-    if (l == 0 && (int)m.pv[pidx] + k == (int)np1) atomicOr(&m.SAT[v >> 5], 1u << (v & 31));
-    bits_store(m.P, P1);
+    if (l == 0 && (int)m.pv()[pidx] + k == (int)np1) atomicOr(&m.SAT()[v >> 5], 1u << (v & 31));
+    bits_store(m.P(), P1);
     __syncwarp();
     // C filter: class >= UNLINK2EQUAL and P' + c a k-plex (isKplex3)
     for (int i = l; i < (int)nc; i += 32) {
-        const uint32_t c = m.list[np + i];
-        if (c == v || !test_bit(m.M2, c)) continue;
-        const int pc = (int)m.pv[np + i] + (int)test_bit(m.ROW, c);
+        const uint32_t c = m.list()[np + i];
+        if (c == v || !test_bit(m.M2(), c)) continue;
+        const int pc = (int)m.pv()[np + i] + (int)test_bit(m.ROW(), c);
         if (pc + k < (int)np1 + 1) continue;
-        if (rowg_covers(A + c * W, m.SAT, W)) atomicOr(&m.NC[c >> 5], 1u << (c & 31));
+        if (rowg_covers(A + c * W, m.SAT(), W)) atomicOr(&m.NC()[c >> 5], 1u << (c & 31));
     }
-    if (l == 0) ww.bb += (unsigned long long)nc * 4ull * W;
+    if (l == 0) ww.bb() += (unsigned long long)nc * 4ull * W;
     __syncwarp();
-    const Bits<NW> C1 = bits_load<NW>(m.NC, 32 * NW);
+    const Bits<NW> C1 = bits_load<NW>(m.NC(), 32 * NW);
     const uint32_t nc1 = (uint32_t)bits_count(C1);
-    bits_store(m.PC, bits_or(P1, C1));
+    bits_store(m.PC(), bits_or(P1, C1));
     __syncwarp();
     // upperBound2 over P' (src:1022-1040)
     bool ub = true;
     for (int i = l; i <= (int)np; i += 32) {
-        const uint32_t u = (i < (int)np) ? m.list[i] : v;
-        if (rowg_popc(A + u * W, m.PC, W) + k < q) ub = false;
+        const uint32_t u = (i < (int)np) ? m.list()[i] : v;
+        if (rowg_popc(A + u * W, m.PC(), W) + k < q) ub = false;
     }
-    if (l == 0) ww.bb += (unsigned long long)np1 * 4ull * W;
+    if (l == 0) ww.bb() += (unsigned long long)np1 * 4ull * W;
     if (!__all_sync(FULL, ub)) return false;
     // X filter: class >= UNLINK2MORE and P' + x a k-plex
-    const int nxl = bits_list(X, m.list);
+    const int nxl = bits_list(X, m.list());
     for (int i = l; i < nxl; i += 32) {
-        const uint32_t x = m.list[i];
-        if (!test_bit(m.M4, x)) continue;
+        const uint32_t x = m.list()[i];
+        if (!test_bit(m.M4(), x)) continue;
         bool ok;
-        const int px = rowg_popc_covers(A + x * W, m.P, m.SAT, W, &ok);
-        if (ok && px + k >= (int)np1 + 1) atomicOr(&m.NX[x >> 5], 1u << (x & 31));
+        const int px = rowg_popc_covers(A + x * W, m.P(), m.SAT(), W, &ok);
+        if (ok && px + k >= (int)np1 + 1) atomicOr(&m.NX()[x >> 5], 1u << (x & 31));
     }
-    if (l == 0) ww.bb += (unsigned long long)nxl * 4ull * W;
+    if (l == 0) ww.bb() += (unsigned long long)nxl * 4ull * W;
     __syncwarp();
-    const Bits<NW> X1 = bits_load<NW>(m.NX, 32 * NW);
+    const Bits<NW> X1 = bits_load<NW>(m.NX(), 32 * NW);
     t->nx = (uint32_t)bits_count(X1);
     t->P = P1; t->C = C1; t->X = X1;
     t->np = np1; t->nc = nc1;
-    if (l == 0) { ++ww.tasks; ww.bb += 12ull * W; }
+    if (l == 0) { ++ww.tasks(); ww.bb() += 12ull * W; }
     return true;
 }
 
@@ -1007,12 +996,11 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
     const uint32_t* A = nullptr;
     uint32_t same_root = 0;
     uint32_t acc_graph = 0;
-    unsigned long long* CT = m.CT;
+    unsigned long long* CT = m.CT();
     if (l < 16) CT[l] = 0ull;
-    if (l < STACK_CACHE) m.SCT[l] = 0xffffffffu;
+    if (l < STACK_CACHE) m.SCT()[l] = 0xffffffffu;
     __syncwarp();
-    WarpWork ww{sp.stacks + (uint64_t)warp * sp.stack_depth * SW, 0ull, 0ull,
-                CT[CT_CNT], CT[CT_HSUM], CT[CT_TASKS], CT[CT_NODES], CT[CT_BB]};
+    WarpWork ww{sp.stacks + (uint64_t)warp * sp.stack_depth * SW, 0ull, 0ull, CT};
     const unsigned long long resume_at = sp.pause_at / 2 > 0 ? sp.pause_at / 2 : 1;
     bool have = false, counted = false, ks_active = false, paused = false, is_idle = false;
     unsigned long long idle = 0;   // idle iterations counted toward spin_limit
@@ -1032,7 +1020,7 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
         if (!have && ww.stop > ww.sbot) {
             --ww.stop;
             const uint32_t cs = (uint32_t)(ww.stop % STACK_CACHE);
-            if (m.SCT[cs] == (uint32_t)ww.stop) load_record<NW>(m.SC + cs * SW, Wt, &t, false);   // still cached
+            if (m.SCT()[cs] == (uint32_t)ww.stop) load_record<NW>(m.SC() + cs * SW, Wt, &t, false);   // still cached
             else load_record<NW>(ww.stack + (ww.stop % sp.stack_depth) * SW, Wt, &t, true);
             have = true;
             __syncwarp();
@@ -1045,7 +1033,7 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
                 if (l == 0) {
                     const uint32_t iw = BQ.idle_warps();
                     if (iw > 0 && BQ.n() < iw) give = 1;
-                    else if ((ww.nodes & 15) == 0 && pool_size(sp) < sp.low_water) give = 2;
+                    else if ((ww.nodes() & 15) == 0 && pool_size(sp) < sp.low_water) give = 2;
                 }
                 give = __shfl_sync(FULL, give, 0);
                 if (give) {
@@ -1063,8 +1051,8 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
                 R = root_view(sp, t.root);
                 cur_root = t.root;
                 if (R.graph != acc_graph) {   // results are kept per input graph
-                    if (l == 0 && (ww.cnt || ww.hsum)) { atomicAdd(&sp.gcount[acc_graph], ww.cnt); atomicAdd(&sp.ghash[acc_graph], ww.hsum); }
-                    if (l == 0) { CT[CT_TOT_CNT] += ww.cnt; CT[CT_TOT_HSUM] += ww.hsum; ww.cnt = ww.hsum = 0; }
+                    if (l == 0 && (ww.cnt() || ww.hsum())) { atomicAdd(&sp.gcount[acc_graph], ww.cnt()); atomicAdd(&sp.ghash[acc_graph], ww.hsum()); }
+                    if (l == 0) { CT[CT_TOT_CNT] += ww.cnt(); CT[CT_TOT_HSUM] += ww.hsum(); ww.cnt() = ww.hsum() = 0; }
                     __syncwarp();
                     acc_graph = R.graph;
                 }
@@ -1073,13 +1061,13 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
             } else if (++same_root == sp.stage_after && R.n * R.W <= sp.a_words) {
                 // the warp keeps working on this root: copy its adjacency rows to shared memory
                 const uint4* src = reinterpret_cast<const uint4*>(R.A);
-                uint4* dst = reinterpret_cast<uint4*>(m.A);
+                uint4* dst = reinterpret_cast<uint4*>(m.A());
                 for (uint32_t i = l; i < R.n * R.W / 4; i += 32) dst[i] = __ldg(src + i);
                 __syncwarp();
-                A = m.A;
+                A = m.A();
                 if (l == 0) ++CT[CT_STAGE];
             }
-            if (l == 0) ++ww.nodes;
+            if (l == 0) ++ww.nodes();
             const long long b0 = clock64();
             have = bnb_node<NW>(sp, m, R, A, &t, ww);
             __syncwarp();
@@ -1138,7 +1126,7 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
                         if (l == 0) ++CT[CT_KS_TASKS];
                         const uint32_t r = S.root();
                         // stage this lane's words in shared memory; the record is hdr | P | C | X
-                        bits_store(m.P, e.P); bits_store(m.NC, e.C); bits_store(m.NX, e.X);
+                        bits_store(m.P(), e.P); bits_store(m.NC(), e.C); bits_store(m.NX(), e.X);
                         __syncwarp();
                         auto word = [&](unsigned i) -> uint32_t {
                             if (i == 0) return r;
@@ -1146,7 +1134,7 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
                             if (i == 2) return e.nx;
                             if (i < 4) return 0u;
                             const unsigned j = i - 4, which = j / Wt, wi = j % Wt;
-                            return which == 0 ? m.P[wi] : (which == 1 ? m.NC[wi] : m.NX[wi]);
+                            return which == 0 ? m.P()[wi] : (which == 1 ? m.NC()[wi] : m.NX()[wi]);
                         };
                         bool pushed = false;
                         if (l == 0) { atomicAdd(&sp.ctr->work, 1u); __threadfence(); }   // the task's unit
@@ -1185,9 +1173,9 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
         // ---------------- consumer: this block's queue, else (one warp per block at a
         // time) the global pool, else refill from the spill ring
         if (!is_idle) { if (l == 0) atomicAdd(BQ.idle(), 1u); is_idle = true; }
-        if (bq_pop(BQ, m.rec)) {   // takes over the record's unit of work
+        if (bq_pop(BQ, m.rec())) {   // takes over the record's unit of work
             wake();
-            load_record<NW>(m.rec, Wt, &t, false);
+            load_record<NW>(m.rec(), Wt, &t, false);
             have = true;
             counted = true;
             if (l == 0) atomicAdd(&sp.ctr->holders, 1u);
@@ -1203,12 +1191,12 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
             }
             which = __shfl_sync(FULL, which, 0);
             if (which) {
-                const bool got = which == 1 ? pool_pop(sp, m.rec) : ring_pop(sp, spill_ring(sp), m.rec);
+                const bool got = which == 1 ? pool_pop(sp, m.rec()) : ring_pop(sp, spill_ring(sp), m.rec());
                 if (l == 0) atomicExch(BQ.poller(), 0);
                 if (got) {
                     wake();
                     if (which == 2 && l == 0) ++CT[CT_REFILL];
-                    load_record<NW>(m.rec, Wt, &t, false);
+                    load_record<NW>(m.rec(), Wt, &t, false);
                     have = true;
                     counted = true;
                     if (l == 0) atomicAdd(&sp.ctr->holders, 1u);
@@ -1248,13 +1236,13 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
     }
     wake();
     if (l == 0) {
-        if (ww.cnt || ww.hsum) { atomicAdd(&sp.gcount[acc_graph], ww.cnt); atomicAdd(&sp.ghash[acc_graph], ww.hsum); }
-        atomicAdd(&sp.ctr->count, CT[CT_TOT_CNT] + ww.cnt);
-        atomicAdd(&sp.ctr->hash, CT[CT_TOT_HSUM] + ww.hsum);
-        atomicAdd(&sp.ctr->tasks, ww.tasks + CT[CT_KS_TASKS]);
+        if (ww.cnt() || ww.hsum()) { atomicAdd(&sp.gcount[acc_graph], ww.cnt()); atomicAdd(&sp.ghash[acc_graph], ww.hsum()); }
+        atomicAdd(&sp.ctr->count, CT[CT_TOT_CNT] + ww.cnt());
+        atomicAdd(&sp.ctr->hash, CT[CT_TOT_HSUM] + ww.hsum());
+        atomicAdd(&sp.ctr->tasks, ww.tasks() + CT[CT_KS_TASKS]);
         atomicAdd(&sp.ctr->ks_tasks, CT[CT_KS_TASKS]);
-        atomicAdd(&sp.ctr->nodes, ww.nodes);
-        atomicAdd(&sp.ctr->bnb_bytes, ww.bb);
+        atomicAdd(&sp.ctr->nodes, ww.nodes());
+        atomicAdd(&sp.ctr->bnb_bytes, ww.bb());
         atomicAdd(&sp.ctr->bnb_done, 1u);
         atomicAdd(&sp.ctr->stage_copies, CT[CT_STAGE]);
         atomicAdd(&sp.ctr->ks_cycles, CT[CT_KS_CYC]);

@@ -217,14 +217,15 @@ def make_params(k: int, q: int, thres: float = 0.25, truss: int = 0, flags: int 
 
 def enumerate_csr(off: np.ndarray, adj: np.ndarray, k: int, q: int, thres: float = 0.25, truss: int = 0,
                   flags: int = FLAG_QUIET, device: int = 0, pool_slots: int = 0, check: bool = True,
-                  shard_index: int = 0, shard_count: int = 0, root_begin: int = 0, root_end: int = 0) -> dict:
+                  shard_index: int = 0, shard_count: int = 0, root_begin: int = 0, root_end: int = 0,
+                  blocks_per_sm: int = 0, stage_after: int = 0) -> dict:
     """Count and hash of the maximal k-plexes with >= q vertices (kplex_enumerate_csr).
     root_begin/root_end (end 0 = all) and shard_index/shard_count restrict the
     search to a stated subset of roots by degeneracy rank."""
     off = np.ascontiguousarray(off, dtype=np.uint32)
     adj = np.ascontiguousarray(adj, dtype=np.uint32)
     p = make_params(k, q, thres, truss, flags, device, pool_slots, 0, shard_index, shard_count,
-                    root_begin=root_begin, root_end=root_end)
+                    blocks_per_sm=blocks_per_sm, stage_after=stage_after, root_begin=root_begin, root_end=root_end)
     r = Result()
     rc = lib().kplex_enumerate_csr(_u32p(off), _u32p(adj), len(off) - 1, len(adj), ctypes.byref(p), ctypes.byref(r))
     if rc and check:
@@ -263,11 +264,12 @@ class Prepared:
 
 def prepare(off: np.ndarray, adj: np.ndarray, k: int, q: int, thres: float = 0.25, truss: int = 0,
             flags: int = FLAG_QUIET, device: int = 0, pool_slots: int = 0, shard_index: int = 0,
-            shard_count: int = 0, root_begin: int = 0, root_end: int = 0) -> Prepared:
+            shard_count: int = 0, root_begin: int = 0, root_end: int = 0, blocks_per_sm: int = 0,
+            stage_after: int = 0) -> Prepared:
     off = np.ascontiguousarray(off, dtype=np.uint32)
     adj = np.ascontiguousarray(adj, dtype=np.uint32)
     p = make_params(k, q, thres, truss, flags, device, pool_slots, 0, shard_index, shard_count,
-                    root_begin=root_begin, root_end=root_end)
+                    blocks_per_sm=blocks_per_sm, stage_after=stage_after, root_begin=root_begin, root_end=root_end)
     h = ctypes.c_void_p()
     r = Result()
     rc = lib().kplex_prepare(_u32p(off), _u32p(adj), len(off) - 1, len(adj), ctypes.byref(p), ctypes.byref(h), ctypes.byref(r))
