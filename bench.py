@@ -524,6 +524,24 @@ def main():
         if pj.get("workload") == cfg["workload"] and "dram_bytes_per_launch" in pj:
             traffic = float(pj["dram_bytes_per_launch"])
 
+    # instruction issue, the resource this latency-bound search actually uses: warp
+    # instructions per branch node from an ncu capture of the same kernel on a root
+    # shard (profiles/search_kernel_issue.txt), times this launch's nodes, against
+    # SMs x 4 schedulers x one instruction per cycle at the sampled SM clock
+    issue = None
+    iprof = os.path.join(ROOT, "profiles", "search_kernel_issue.txt")
+    if os.path.exists(iprof) and clocks and bnb_ms > 0:
+        with open(iprof) as f:
+            ij = dict(line.split(":", 1) for line in f if ":" in line and not line.startswith("#"))
+        ij = {k.strip(): v.strip() for k, v in ij.items()}
+        if ij.get("workload") == cfg["workload"] and "inst_per_node" in ij:
+            sms = torch.cuda.get_device_properties(local).multi_processor_count
+            inst = float(ij["inst_per_node"]) * res[-1]["nodes"]
+            cyc = (bnb_ms / max(bnb_launches, 1)) * 1e-3 * clocks["sm_mhz"] * 1e6
+            issue = {"inst_per_node": float(ij["inst_per_node"]), "inst_per_launch": inst,
+                     "issue_slots_per_launch": sms * 4 * cyc, "frac": inst / (sms * 4 * cyc),
+                     "source": "profiles/search_kernel_issue.txt (" + ij.get("capture", "") + ")"}
+
     line = {
         "metric": METRIC,
         "value": total_count * args.steps / (dev_ms_max / 1e3) if dev_ms_max > 0 else 0.0,
@@ -533,10 +551,13 @@ def main():
         "data": data_kind(cfg),
         "config": cfg,
         "count": total_count, "hash": f"{total_hash:#018x}", "results_consistent": consistent,
-        "roofline": {"bound": "hbm", "kernel": "bnb_kernel", "achieved": achieved, "peak": peak,
+        "roofline": {"bound": "hbm", "kernel": "search_kernel", "achieved": achieved, "peak": peak,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak if peak else 0.0,
                      "traffic": traffic, "bytes_per_launch": bnb_bytes / max(bnb_launches, 1),
-                     "ms_per_launch": bnb_ms / max(bnb_launches, 1)},
+                     "ms_per_launch": bnb_ms / max(bnb_launches, 1),
+                     # the search runs from L1, shared memory and L2 (traffic is about 1/30,000 of the
+                     # algorithmic bytes): the limiter is instruction issue, not HBM
+                     "limiter": "issue", "issue": issue},
         "e2e": {"value": e2e_total / (e2e_max / 1e3) if e2e_max > 0 else 0.0, "unit": UNIT,
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 512, "ms_per_step": e2e_max, "parts": e2e_parts},
         "gpu_launches": launches,

@@ -12,13 +12,16 @@ def _dense(orc):
     return orc.random_graph(80, 0.15, 3, [(20, 0.9), (18, 0.95), (16, 1.0)])
 
 
+@pytest.mark.parametrize("k,q", [(3, 8), (4, 9)])
 @pytest.mark.parametrize("slots,thres", [(64, 0.5), (256, 0.25), (4096, 1.0)])
-def test_pause_resume_same_result(kp, orc, slots, thres):
-    """A tiny task pool forces k-search to pause many times; results do not change (host:1094-1122)."""
+def test_pause_resume_same_result(kp, orc, slots, thres, k, q):
+    """A tiny task pool forces k-search to pause many times; results do not change
+    (host:1094-1122) and equal the oracle's, task count included (with k >= 3 the
+    k-search job split reorders C2, which the oracle mirrors)."""
     off, adj = _dense(orc)
-    full = kp.enumerate_csr(off, adj, 3, 8)
-    g = kp.enumerate_csr(off, adj, 3, 8, thres=thres, pool_slots=slots)
-    assert (g["count"], g["hash"], g["tasks"]) == (full["count"], full["hash"], full["tasks"])
+    o = orc.enumerate_csr(off, adj, k, q, threads=4)
+    g = kp.enumerate_csr(off, adj, k, q, thres=thres, pool_slots=slots)
+    assert (g["count"], g["hash"], g["tasks"]) == (o["count"], o["hash"], o["tasks"])
     if slots == 64:
         assert g["pauses"] > 0
 
@@ -66,10 +69,13 @@ def test_spill_to_host_same_result(kp, orc, slots):
     memory instead of pausing k-search; idle warps refill from it.  The
     enumeration is unchanged (the reference's spill/refill, host:168-251, is dead code)."""
     off, adj = _dense(orc)
-    full = kp.enumerate_csr(off, adj, 3, 8)
+    o = orc.enumerate_csr(off, adj, 3, 8, threads=4)
     g = kp.enumerate_csr(off, adj, 3, 8, thres=0.25, pool_slots=slots, flags=kp.FLAG_QUIET | kp.FLAG_SPILL_HOST)
-    assert (g["count"], g["hash"], g["tasks"]) == (full["count"], full["hash"], full["tasks"])
+    assert (g["count"], g["hash"], g["tasks"]) == (o["count"], o["hash"], o["tasks"])
     assert g["spilled"] > 0
+    o4 = orc.enumerate_csr(off, adj, 4, 9, threads=4)
+    g4 = kp.enumerate_csr(off, adj, 4, 9, thres=0.25, pool_slots=slots, flags=kp.FLAG_QUIET | kp.FLAG_SPILL_HOST)
+    assert (g4["count"], g4["hash"], g4["tasks"]) == (o4["count"], o4["hash"], o4["tasks"])
     w = kp.WORKLOADS["small"]
     so, sa = kp.workload_graph("small")
     a = kp.enumerate_csr(so, sa, w["k"], w["q"], pool_slots=64, flags=kp.FLAG_QUIET | kp.FLAG_SPILL_HOST)
