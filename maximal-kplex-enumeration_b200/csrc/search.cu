@@ -218,6 +218,7 @@ __device__ void ks_start(const SearchParams& sp, const KsSlot<NW>& S, uint32_t r
     for (int j = 0; j < NW; ++j) {
         const uint32_t wi = l + 32u * j, lo = wi * 32;
         uint32_t c1 = 0, x = 0;
+        #pragma unroll 1
         for (uint32_t b = 0; b < 32; ++b) {
             const uint32_t v = lo + b;
             if (v >= 1 && v < hop) c1 |= 1u << b;
@@ -227,6 +228,7 @@ __device__ void ks_start(const SearchParams& sp, const KsSlot<NW>& S, uint32_t r
         S.xbits()[wi] = x;
         S.pbits()[wi] = (wi == 0) ? 1u : 0u;
     }
+    #pragma unroll 1
     for (uint32_t i = l; i < n; i += 32) {
         if (i >= hop && i < hop + keep) S.c2()[i - hop] = (uint16_t)i;
         S.t1()[i] = 0;
@@ -252,6 +254,7 @@ __device__ bool ks_upper_bound(const SearchParams& sp, const RootView& R, const 
     bits_store(S.mask(), PC1);
     __syncwarp();
     bool ok = true;
+    #pragma unroll 1
     for (uint32_t i = l; i < np; i += 32) {
         const uint32_t u = S.P()[i];
         if (row_and_popc(R.A + (uint64_t)u * R.W, S.mask(), R.W) + R.k < R.q) ok = false;
@@ -296,6 +299,7 @@ __device__ int ks_advance(const SearchParams& sp, const KsSlot<NW>& S, Emitted<N
     auto update23 = [&](uint32_t node, uint16_t tag) {   // updateCand23, src:1099-1122 (order preserving)
         const uint32_t* m2row = R.M2() + (uint64_t)node * W;
         uint32_t write = 0;
+        #pragma unroll 1
         for (uint32_t b = 0; b < nc2; b += 32) {
             const uint32_t i = b + l;
             uint16_t v = 0;
@@ -391,15 +395,18 @@ __device__ int ks_advance(const SearchParams& sp, const KsSlot<NW>& S, Emitted<N
                 bits_fill<NW>(S.aux(), 0u);
                 bits_fill<NW>(S.keep(), 0u);
                 __syncwarp();
+                #pragma unroll 1
                 for (uint32_t i = l; i < np; i += 32) {
                     const uint32_t v = S.P()[i];
                     if (row_and_popc(R.A + (uint64_t)v * W, S.mask(), W) + k == (int)np) atomicOr(&S.aux()[v >> 5], 1u << (v & 31));
                 }
                 const int m1 = bits_list(C1, S.lst());
+                #pragma unroll 1
                 for (int i = l; i < m1; i += 32) {
                     const uint32_t v = S.lst()[i];
                     const uint32_t* row = R.A + (uint64_t)v * W;
                     bool ok = row_and_popc(row, S.mask(), W) + k >= (int)np + 1;
+                    #pragma unroll 1
                     for (uint32_t w = 0; ok && w < W; ++w) if (S.aux()[w] & ~__ldg(row + w)) ok = false;
                     if (ok) atomicOr(&S.keep()[v >> 5], 1u << (v & 31));
                 }
@@ -411,12 +418,14 @@ __device__ int ks_advance(const SearchParams& sp, const KsSlot<NW>& S, Emitted<N
             continue;
         }
         // st == 5: undo this frame (src:2405-2441)
+        #pragma unroll 1
         for (uint32_t i = 0; i < br; ++i) {
             const uint32_t node = S.P()[np - 1];
             --np;
             bits_clear(P, node);
             c2_push(node);
         }
+        #pragma unroll 1
         for (uint32_t b = 0; b < n; b += 32) {
             const uint32_t i = b + l;
             bool h1 = false, h2 = false;
@@ -452,6 +461,7 @@ __device__ __forceinline__ int rowg_popc(const uint32_t* row, const uint32_t* ma
     int c = 0;
     const uint4* r4 = reinterpret_cast<const uint4*>(row);
     const uint4* m4 = reinterpret_cast<const uint4*>(mask);
+#pragma unroll 1
     for (unsigned w = 0; w < W / 4; ++w) {
         const uint4 a = r4[w], m = m4[w];
         c += __popc(a.x & m.x) + __popc(a.y & m.y) + __popc(a.z & m.z) + __popc(a.w & m.w);
@@ -466,6 +476,7 @@ __device__ __forceinline__ int rowg_popc_covers(const uint32_t* row, const uint3
     const uint4* r4 = reinterpret_cast<const uint4*>(row);
     const uint4* m4 = reinterpret_cast<const uint4*>(mask);
     const uint4* s4 = reinterpret_cast<const uint4*>(sat);
+#pragma unroll 1
     for (unsigned w = 0; w < W / 4; ++w) {
         const uint4 a = r4[w], m = m4[w], t = s4[w];
         c += __popc(a.x & m.x) + __popc(a.y & m.y) + __popc(a.z & m.z) + __popc(a.w & m.w);
@@ -480,6 +491,7 @@ __device__ __forceinline__ bool rowg_covers(const uint32_t* row, const uint32_t*
     uint32_t miss = 0;
     const uint4* r4 = reinterpret_cast<const uint4*>(row);
     const uint4* s4 = reinterpret_cast<const uint4*>(sat);
+#pragma unroll 1
     for (unsigned w = 0; w < W / 4; ++w) {
         const uint4 a = r4[w], t = s4[w];
         miss |= (t.x & ~a.x) | (t.y & ~a.y) | (t.z & ~a.z) | (t.w & ~a.w);
@@ -494,6 +506,7 @@ __device__ __forceinline__ void rowg_popc2(const uint32_t* row, const uint32_t* 
     const uint4* r4 = reinterpret_cast<const uint4*>(row);
     const uint4* x4 = reinterpret_cast<const uint4*>(m1);
     const uint4* y4 = reinterpret_cast<const uint4*>(m2);
+#pragma unroll 1
     for (unsigned w = 0; w < W / 4; ++w) {
         const uint4 a = r4[w], x = x4[w], y = y4[w];
         a1 += __popc(a.x & x.x) + __popc(a.y & x.y) + __popc(a.z & x.z) + __popc(a.w & x.w);
@@ -575,8 +588,10 @@ __device__ __forceinline__ void pivot_tree(int& m, int& v, int& p, int& idx) {
 // root's left set extends S (list[0..s), degrees deg[], bitset sS) to a k-plex.
 // Candidates must be adjacent to every saturated member of S and to one of any
 // k members; each candidate's count is its popcount against S.
-__device__ bool left_maximal(const SearchParams& sp, const RootView& R, const BnbSmem& m, int s, const uint16_t* deg,
-                             const uint32_t* sS, unsigned long long& bb) {
+// Out of line (with its arguments by value): it runs only at the leaves, and
+// keeping it out of the node loop keeps that loop's code small.
+__device__ __noinline__ bool left_maximal(const RootView R, const BnbSmem m, int s, const uint16_t* deg,
+                                          const uint32_t* sS, unsigned long long* bb) {
     const unsigned l = lane_id();
     const int k = R.k;
     if (R.nleft == 0) return true;
@@ -584,6 +599,7 @@ __device__ bool left_maximal(const SearchParams& sp, const RootView& R, const Bn
     int nrows = 0;
     bool found = false;
     // the left set's words in chunks of 32, one word per lane
+    #pragma unroll 1
     for (uint32_t base = 0; base < WL && !found; base += 32) {
         const uint32_t w = base + l;
         uint32_t lc = 0;
@@ -591,6 +607,7 @@ __device__ bool left_maximal(const SearchParams& sp, const RootView& R, const Bn
             const int lo = (int)w * 32, nl = (int)R.nleft;
             lc = nl >= lo + 32 ? FULL : (nl > lo ? ((1u << (nl - lo)) - 1) : 0u);
         }
+        #pragma unroll 1
         for (int b = 0; b < s; b += 32) {   // adjacent to every saturated member
             const int i = b + (int)l;
             const bool sat = i < s && (int)deg[i] + k <= s;
@@ -603,6 +620,7 @@ __device__ bool left_maximal(const SearchParams& sp, const RootView& R, const Bn
             }
         }
         uint32_t un = 0;   // and to one of any k members
+        #pragma unroll 1
         for (int t = 0; t < k && t < s; ++t) {
             const uint32_t u = m.list()[t];
             if (w < WL) un |= __ldg(R.LA() + (uint64_t)u * WL + w);
@@ -621,19 +639,20 @@ __device__ bool left_maximal(const SearchParams& sp, const RootView& R, const Bn
         found = __any_sync(FULL, f);
     }
     nrows = warp_sum(nrows);
-    if (l == 0) bb += (unsigned long long)nrows * 4ull * W + (unsigned long long)(k + 1) * 4ull * WL;
+    if (l == 0) *bb += (unsigned long long)nrows * 4ull * W + (unsigned long long)(k + 1) * 4ull * WL;
     return !found;
 }
 
 // Adds one maximal k-plex (list[0..s)) to the count and hash.
 template <int NW>
-__device__ void emit_plex(const SearchParams& sp, const RootView& R, const BnbSmem& m, int s,
-                          unsigned long long& cnt, unsigned long long& hsum) {
+__device__ __noinline__ void emit_plex(const RootView R, const BnbSmem m, int s, uint32_t hash_on,
+                                       unsigned long long* cnt, unsigned long long* hsum) {
     const unsigned l = lane_id();
-    if (l == 0) ++cnt;
-    if (!sp.hash_on) return;
+    if (l == 0) ++*cnt;
+    if (!hash_on) return;
     bits_fill<NW>(m.SB(), 0u);
     __syncwarp();
+    #pragma unroll 1
     for (int i = l; i < s; i += 32) {
         const uint32_t rk = __ldg(R.srank() + m.list()[i]);
         atomicOr(&m.SB()[rk >> 5], 1u << (rk & 31));
@@ -656,7 +675,7 @@ __device__ void emit_plex(const SearchParams& sp, const RootView& R, const BnbSm
             x = __shfl_sync(FULL, x, L);
         }
     }
-    if (l == 0) hsum += x;
+    if (l == 0) *hsum += x;
 }
 
 template <int NW>
@@ -699,6 +718,7 @@ __device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootVie
     bits_list(P, m.list());
     bits_list(C, m.list() + np);
     const int tot = (int)(np + nc);
+    #pragma unroll 1
     for (int i = l; i < tot; i += 32) {
         int g, p;
         rowg_popc2(A + (uint32_t)m.list()[i] * W, m.PC(), m.P(), W, g, p);
@@ -708,12 +728,13 @@ __device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootVie
     if (l == 0) ww.bb() += (unsigned long long)(tot + 3) * 4ull * W;   // rows + the record's P, C, X
     __syncwarp();
     if (nc == 0) {   // src:1579-1588
-        if (nx == 0 && (int)np >= q && left_maximal(sp, R, m, (int)np, m.pv(), m.P(), ww.bb()))
-            emit_plex<NW>(sp, R, m, (int)np, ww.cnt(), ww.hsum());
+        if (nx == 0 && (int)np >= q && left_maximal(R, m, (int)np, m.pv(), m.P(), &ww.bb()))
+            emit_plex<NW>(R, m, (int)np, sp.hash_on, &ww.cnt(), &ww.hsum());
         return false;
     }
     // pivot in P: minimum neiInG, ties to the smaller index (src:1592-1620)
     unsigned long long key = ~0ull;   // (neiInG, vertex, neiInP) of this lane's best P member
+    #pragma unroll 1
     for (int i = l; i < (int)np; i += 32) {
         const unsigned long long kk = ((unsigned long long)m.gv()[i] << 32) | ((unsigned long long)m.list()[i] << 16) | m.pv()[i];
         key = kk < key ? kk : key;
@@ -732,6 +753,7 @@ __device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootVie
         bits_store(m.ROW(), bits_load<NW>(A + (uint32_t)pp * W, W));
         __syncwarp();
         pmin = INT_MAX; piv = -1; pval = 0; pidx = -1;
+        #pragma unroll 1
         for (int i = l; i < (int)nc; i += 32) {
             const uint32_t v = m.list()[np + i];
             if (test_bit(m.ROW(), v)) continue;
@@ -743,6 +765,7 @@ __device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootVie
     } else {
         // minimum over P (seeded) and C (src:1669-1697)
         pmin = minP; piv = pp; pval = ppP; pidx = -2;
+        #pragma unroll 1
         for (int i = l; i < (int)nc; i += 32) {
             const uint32_t v = m.list()[np + i];
             const int g = m.gv()[np + i], p = m.pv()[np + i];
@@ -754,21 +777,24 @@ __device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootVie
             // P ∪ C is a k-plex (src:1698-1717)
             if (tot < q) return false;
             const int nxl = bits_list(X, m.list() + tot);
+            #pragma unroll 1
             for (int i = l; i < nxl; i += 32)
                 m.gv()[tot + i] = (uint16_t)rowg_popc(A + (uint32_t)m.list()[tot + i] * W, m.PC(), W);
             bits_fill<NW>(m.SAT(), 0u);
             __syncwarp();
+            #pragma unroll 1
             for (int i = l; i < tot; i += 32)
                 if ((int)m.gv()[i] + k == tot) { const uint32_t u = m.list()[i]; atomicOr(&m.SAT()[u >> 5], 1u << (u & 31)); }
             __syncwarp();
             bool ext = false;
+            #pragma unroll 1
             for (int i = l; i < nxl; i += 32) {   // isKplexPC2 src:601-622
                 if ((int)m.gv()[tot + i] + k < tot + 1) continue;
                 ext |= rowg_covers(A + (uint32_t)m.list()[tot + i] * W, m.SAT(), W);
             }
             if (l == 0) ww.bb() += (unsigned long long)nxl * 4ull * W;
             if (__any_sync(FULL, ext)) return false;
-            if (left_maximal(sp, R, m, tot, m.gv(), m.PC(), ww.bb())) emit_plex<NW>(sp, R, m, tot, ww.cnt(), ww.hsum());
+            if (left_maximal(R, m, tot, m.gv(), m.PC(), &ww.bb())) emit_plex<NW>(R, m, tot, sp.hash_on, &ww.cnt(), &ww.hsum());
             return false;
         }
     }
@@ -811,6 +837,7 @@ __device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootVie
     bits_fill<NW>(m.NX(), 0u);
     __syncwarp();
     // saturated members of P + v: neiInP' + k == |P'|
+    #pragma unroll 1
     for (int i = l; i < (int)np; i += 32) {
         const uint32_t u = m.list()[i];
         const int pu = (int)m.pv()[i] + (int)test_bit(m.ROW(), u);
@@ -820,6 +847,7 @@ __device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootVie
     bits_store(m.P(), P1);
     __syncwarp();
     // C filter: class >= UNLINK2EQUAL and P' + c a k-plex (isKplex3)
+    #pragma unroll 1
     for (int i = l; i < (int)nc; i += 32) {
         const uint32_t c = m.list()[np + i];
         if (c == v || !test_bit(m.M2(), c)) continue;
@@ -835,6 +863,7 @@ __device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootVie
     __syncwarp();
     // upperBound2 over P' (src:1022-1040)
     bool ub = true;
+    #pragma unroll 1
     for (int i = l; i <= (int)np; i += 32) {
         const uint32_t u = (i < (int)np) ? m.list()[i] : v;
         if (rowg_popc(A + u * W, m.PC(), W) + k < q) ub = false;
@@ -843,6 +872,7 @@ __device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootVie
     if (!__all_sync(FULL, ub)) return false;
     // X filter: class >= UNLINK2MORE and P' + x a k-plex
     const int nxl = bits_list(X, m.list());
+    #pragma unroll 1
     for (int i = l; i < nxl; i += 32) {
         const uint32_t x = m.list()[i];
         if (!test_bit(m.M4(), x)) continue;
@@ -925,6 +955,7 @@ struct BlockQueue {
 
 // lane 0 only; a bounded spin (the lock is held for one record copy)
 __device__ __forceinline__ bool bq_lock(const BlockQueue& q) {
+    #pragma unroll 1
     for (int i = 0; i < 1 << 14; ++i) {
         if (atomicCAS(q.lock(), 0, 1) == 0) { __threadfence_block(); return true; }
         __nanosleep(32);
@@ -949,6 +980,7 @@ __device__ bool bq_push(const BlockQueue& q, WordFn word) {
     slot = __shfl_sync(FULL, slot, 0);
     if (slot < 0) return false;
     uint32_t* dst = q.rec((uint32_t)slot);
+    #pragma unroll 1
     for (unsigned i = l; i < q.SW; i += 32) dst[i] = word(i);
     __threadfence_block();
     __syncwarp();
@@ -969,6 +1001,7 @@ __device__ bool bq_pop(const BlockQueue& q, uint32_t* dst) {
     slot = __shfl_sync(FULL, slot, 0);
     if (slot < 0) return false;
     const uint32_t* src = q.rec((uint32_t)slot);
+    #pragma unroll 1
     for (unsigned i = l; i < q.SW; i += 32) dst[i] = src[i];
     __threadfence_block();
     __syncwarp();
@@ -1062,6 +1095,7 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
                 // the warp keeps working on this root: copy its adjacency rows to shared memory
                 const uint4* src = reinterpret_cast<const uint4*>(R.A);
                 uint4* dst = reinterpret_cast<uint4*>(m.A());
+                #pragma unroll 1
                 for (uint32_t i = l; i < R.n * R.W / 4; i += 32) dst[i] = __ldg(src + i);
                 __syncwarp();
                 A = m.A();

@@ -63,6 +63,7 @@ __device__ __forceinline__ int row_and_popc(const uint32_t* __restrict__ row, co
     int c = 0;
     const uint4* r4 = reinterpret_cast<const uint4*>(row);
     const uint4* m4 = reinterpret_cast<const uint4*>(mask);
+#pragma unroll 1
     for (unsigned w = 0; w < W / 4; ++w) {
         const uint4 a = __ldg(r4 + w), m = m4[w];
         c += __popc(a.x & m.x) + __popc(a.y & m.y) + __popc(a.z & m.z) + __popc(a.w & m.w);
