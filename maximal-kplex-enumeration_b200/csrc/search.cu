@@ -967,9 +967,8 @@ __device__ __forceinline__ void bq_unlock(const BlockQueue& q) {
     atomicExch(q.lock(), 0);
 }
 
-// Pushes one record (word(i) for i < SW) if the queue has room; whole warp.
-template <typename WordFn>
-__device__ bool bq_push(const BlockQueue& q, WordFn word) {
+// Pushes one record (SW words from src) if the queue has room; whole warp.
+__device__ __noinline__ bool bq_push(const BlockQueue q, const uint32_t* src, int src_global) {
     const unsigned l = lane_id();
     int slot = -1;
     if (l == 0 && q.n() < BQ_RECORDS && bq_lock(q)) {
@@ -980,8 +979,7 @@ __device__ bool bq_push(const BlockQueue& q, WordFn word) {
     slot = __shfl_sync(FULL, slot, 0);
     if (slot < 0) return false;
     uint32_t* dst = q.rec((uint32_t)slot);
-    #pragma unroll 1
-    for (unsigned i = l; i < q.SW; i += 32) dst[i] = word(i);
+    for (unsigned i = l; i < q.SW; i += 32) dst[i] = rec_word(src, src_global, i);
     __threadfence_block();
     __syncwarp();
     if (l == 0) { *(volatile uint32_t*)q.count() = (uint32_t)slot + 1; bq_unlock(q); }
@@ -990,7 +988,7 @@ __device__ bool bq_push(const BlockQueue& q, WordFn word) {
 }
 
 // Pops the newest record into dst (shared memory, SW words); whole warp.
-__device__ bool bq_pop(const BlockQueue& q, uint32_t* dst) {
+__device__ __noinline__ bool bq_pop(const BlockQueue q, uint32_t* dst) {
     const unsigned l = lane_id();
     int slot = -1;
     if (l == 0 && q.n() > 0 && bq_lock(q)) {
@@ -1071,11 +1069,10 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
                 give = __shfl_sync(FULL, give, 0);
                 if (give) {
                     const uint32_t* src = ww.stack + (ww.sbot % sp.stack_depth) * SW;
-                    auto word = [&](unsigned i) { return __ldcg(src + i); };
                     // the record becomes a unit of work before it can be seen (and taken)
                     if (l == 0) { atomicAdd(&sp.ctr->work, 1u); __threadfence(); }
                     __syncwarp();
-                    const bool ok = (give == 1) ? bq_push(BQ, word) : pool_push(sp, word);
+                    const bool ok = (give == 1) ? bq_push(BQ, src, 1) : pool_push(sp, src, 1);
                     if (ok) ++ww.sbot;
                     else if (l == 0) atomicSub(&sp.ctr->work, 1u);
                 }
@@ -1159,28 +1156,26 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
                     if (got) {
                         if (l == 0) ++CT[CT_KS_TASKS];
                         const uint32_t r = S.root();
-                        // stage this lane's words in shared memory; the record is hdr | P | C | X
-                        bits_store(m.P(), e.P); bits_store(m.NC(), e.C); bits_store(m.NX(), e.X);
+                        // stage the record (hdr | P | C | X) in shared memory, then hand it over
+                        uint32_t* rec = m.rec();
+                        if (l == 0) { rec[0] = r; rec[1] = e.np | (e.nc << 16); rec[2] = e.nx; rec[3] = 0u; }
+#pragma unroll
+                        for (int j = 0; j < NW; ++j) {
+                            const uint32_t wi = l + 32u * j;
+                            if (wi < Wt) { rec[4 + wi] = e.P.w[j]; rec[4 + Wt + wi] = e.C.w[j]; rec[4 + 2 * Wt + wi] = e.X.w[j]; }
+                        }
                         __syncwarp();
-                        auto word = [&](unsigned i) -> uint32_t {
-                            if (i == 0) return r;
-                            if (i == 1) return e.np | (e.nc << 16);
-                            if (i == 2) return e.nx;
-                            if (i < 4) return 0u;
-                            const unsigned j = i - 4, which = j / Wt, wi = j % Wt;
-                            return which == 0 ? m.P()[wi] : (which == 1 ? m.NC()[wi] : m.NX()[wi]);
-                        };
                         bool pushed = false;
                         if (l == 0) { atomicAdd(&sp.ctr->work, 1u); __threadfence(); }   // the task's unit
                         __syncwarp();
                         int local = 0;   // an idle warp of this block takes it directly
                         if (l == 0) local = BQ.idle_warps() > BQ.n();
-                        if (__shfl_sync(FULL, local, 0)) pushed = bq_push(BQ, word);
+                        if (__shfl_sync(FULL, local, 0)) pushed = bq_push(BQ, rec, 0);
                         if (!pushed && to_host) {   // spill: the record goes to pinned host memory
-                            pushed = ring_push(sp, spill_ring(sp), word);
+                            pushed = ring_push(sp, spill_ring(sp), rec, 0);
                             if (pushed && l == 0) ++CT[CT_SPILL];
                         }
-                        if (!pushed) pushed = pool_push(sp, word);
+                        if (!pushed) pushed = pool_push(sp, rec, 0);
                         if (!pushed) {   // ring full: keep the task
                             t.root = r; t.np = e.np; t.nc = e.nc; t.nx = e.nx;
                             t.P = e.P; t.C = e.C; t.X = e.X;

@@ -87,18 +87,24 @@ struct Ring {
 __device__ __forceinline__ Ring main_ring(const SearchParams& sp) { return Ring{sp.pool, sp.pool_seq, sp.pool_data, 0}; }
 __device__ __forceinline__ Ring spill_ring(const SearchParams& sp) { return Ring{sp.spill_pool, sp.spill_seq, sp.spill_data, 1}; }
 
-// Enqueue one record (slot_words words; lane l supplies words l, l+32, ...
-// through `word(i)`).  Returns false when the ring is full or the bounded
-// retry loop gives up; the caller keeps the record.
-template <typename WordFn>
-__device__ inline bool ring_push(const SearchParams& sp, const Ring& r, WordFn word) {
+// Word i of a record: from global memory at L2 (it may have been written by
+// another SM) or from shared memory.
+__device__ __forceinline__ uint32_t rec_word(const uint32_t* src, int src_global, unsigned i) {
+    return src_global ? __ldcg(src + i) : src[i];
+}
+
+// Enqueue one record of slot_words words copied from src.  Returns false when
+// the ring is full or the bounded retry loop gives up; the caller keeps the
+// record.  Out of line: it runs per handed-over task, not per branch node.
+static __device__ __noinline__ bool ring_push(Ring r, uint32_t slot_words, unsigned long long spin_limit, uint32_t test_stuck,
+                                       Counters* ctr, const uint32_t* src, int src_global) {
     Pool* pool = r.ctl;
     const unsigned l = lane_id();
     unsigned long long pos = 0;
     int ok = 0;
     if (l == 0) {
         const unsigned long long cap = pool->cap;
-        for (unsigned long long it = 0; it < sp.spin_limit; ++it) {
+        for (unsigned long long it = 0; it < spin_limit; ++it) {
             pos = atomicAdd(&pool->tail, 0ull);
             const uint32_t seq = atomicAdd(&r.seq[pos % cap], 0u);
             const int dif = (int)(seq - (uint32_t)pos);
@@ -112,14 +118,14 @@ __device__ inline bool ring_push(const SearchParams& sp, const Ring& r, WordFn w
     ok = __shfl_sync(FULL, ok, 0);
     if (!ok) return false;
     pos = __shfl_sync(FULL, pos, 0);
-    if (sp.test_stuck) {   // failure-detection test: claim the slot but never publish it
+    if (test_stuck) {   // failure-detection test: claim the slot but never publish it
         int stuck = 0;
-        if (l == 0) stuck = atomicCAS(&sp.ctr->stuck_once, 0u, 1u) == 0u;
+        if (l == 0) stuck = atomicCAS(&ctr->stuck_once, 0u, 1u) == 0u;
         if (__shfl_sync(FULL, stuck, 0)) return true;
     }
     const unsigned long long slot = pos % pool->cap;
-    uint32_t* dst = r.data + slot * sp.slot_words;
-    for (unsigned i = l; i < sp.slot_words; i += 32) __stcg(dst + i, word(i));
+    uint32_t* dst = r.data + slot * slot_words;
+    for (unsigned i = l; i < slot_words; i += 32) __stcg(dst + i, rec_word(src, src_global, i));
     if (r.sys) __threadfence_system(); else __threadfence();
     __syncwarp();
     if (l == 0) atomicExch(&r.seq[slot], (uint32_t)(pos + 1));
@@ -128,14 +134,14 @@ __device__ inline bool ring_push(const SearchParams& sp, const Ring& r, WordFn w
 
 // Dequeue one record into dst (slot_words words).  Returns false if the ring
 // looks empty (a record still being published counts as empty).
-__device__ inline bool ring_pop(const SearchParams& sp, const Ring& r, uint32_t* dst) {
+static __device__ __noinline__ bool ring_pop(Ring r, uint32_t slot_words, unsigned long long spin_limit, uint32_t* dst) {
     Pool* pool = r.ctl;
     const unsigned l = lane_id();
     unsigned long long pos = 0;
     int ok = 0;
     if (l == 0) {
         const unsigned long long cap = pool->cap;
-        for (unsigned long long it = 0; it < sp.spin_limit; ++it) {
+        for (unsigned long long it = 0; it < spin_limit; ++it) {
             pos = atomicAdd(&pool->head, 0ull);
             const uint32_t seq = atomicAdd(&r.seq[pos % cap], 0u);
             const int dif = (int)(seq - (uint32_t)(pos + 1));
@@ -152,8 +158,8 @@ __device__ inline bool ring_pop(const SearchParams& sp, const Ring& r, uint32_t*
     const unsigned long long cap = pool->cap;
     const unsigned long long slot = pos % cap;
     __threadfence();
-    const uint32_t* src = r.data + slot * sp.slot_words;
-    for (unsigned i = l; i < sp.slot_words; i += 32) dst[i] = __ldcg(src + i);
+    const uint32_t* src = r.data + slot * slot_words;
+    for (unsigned i = l; i < slot_words; i += 32) dst[i] = __ldcg(src + i);
     __threadfence();
     __syncwarp();
     if (l == 0) atomicExch(&r.seq[slot], (uint32_t)(pos + cap));
@@ -166,9 +172,16 @@ __device__ __forceinline__ unsigned long long ring_size(const Ring& r) {
     return t > h ? t - h : 0ull;
 }
 
-template <typename WordFn>
-__device__ inline bool pool_push(const SearchParams& sp, WordFn word) { return ring_push(sp, main_ring(sp), word); }
-__device__ inline bool pool_pop(const SearchParams& sp, uint32_t* dst) { return ring_pop(sp, main_ring(sp), dst); }
+__device__ __forceinline__ bool ring_push(const SearchParams& sp, const Ring& r, const uint32_t* src, int src_global) {
+    return ring_push(r, sp.slot_words, sp.spin_limit, sp.test_stuck, sp.ctr, src, src_global);
+}
+__device__ __forceinline__ bool ring_pop(const SearchParams& sp, const Ring& r, uint32_t* dst) {
+    return ring_pop(r, sp.slot_words, sp.spin_limit, dst);
+}
+__device__ __forceinline__ bool pool_push(const SearchParams& sp, const uint32_t* src, int src_global) {
+    return ring_push(sp, main_ring(sp), src, src_global);
+}
+__device__ __forceinline__ bool pool_pop(const SearchParams& sp, uint32_t* dst) { return ring_pop(sp, main_ring(sp), dst); }
 __device__ __forceinline__ unsigned long long pool_size(const SearchParams& sp) { return ring_size(main_ring(sp)); }
 __device__ __forceinline__ unsigned long long spill_size(const SearchParams& sp) { return sp.spill_on ? ring_size(spill_ring(sp)) : 0ull; }
 
