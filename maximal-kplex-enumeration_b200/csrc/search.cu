@@ -801,6 +801,11 @@ __device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootVie
     // ---------------- branch on piv (src:1197-1465)
     if (piv < 0 || pidx < 0) { if (l == 0) raise_error(sp.ctr, KPLEX_ERR_INTERNAL); return false; }
     const uint32_t v = (uint32_t)piv;
+    // the include child's rows of v, loaded now so that their latency overlaps the
+    // exclude child's write
+    const Bits<NW> rowA = bits_load<NW>(A + v * W, W);
+    const Bits<NW> rowM2 = bits_ldg<NW>(R.M2() + (uint64_t)v * W, W);
+    const Bits<NW> rowM4 = bits_ldg<NW>(R.M4() + (uint64_t)v * W, W);
     {   // exclude child -> this warp's stack
         if (ww.stop - ww.sbot >= sp.stack_depth) { if (l == 0) raise_error(sp.ctr, KPLEX_ERR_INTERNAL); return false; }
         uint32_t* dst = ww.stack + (ww.stop % sp.stack_depth) * SW;
@@ -829,9 +834,9 @@ __device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootVie
     const uint32_t np1 = np + 1;
     Bits<NW> P1 = P;
     bits_set(P1, v);
-    bits_store(m.ROW(), bits_load<NW>(A + v * W, W));
-    bits_store(m.M2(), bits_ldg<NW>(R.M2() + (uint64_t)v * W, W));
-    bits_store(m.M4(), bits_ldg<NW>(R.M4() + (uint64_t)v * W, W));
+    bits_store(m.ROW(), rowA);
+    bits_store(m.M2(), rowM2);
+    bits_store(m.M4(), rowM4);
     bits_fill<NW>(m.SAT(), 0u);
     bits_fill<NW>(m.NC(), 0u);
     bits_fill<NW>(m.NX(), 0u);
