@@ -973,7 +973,7 @@ __device__ __forceinline__ void bq_unlock(const BlockQueue& q) {
 }
 
 // Pushes one record (SW words from src) if the queue has room; whole warp.
-__device__ __noinline__ bool bq_push(const BlockQueue q, const uint32_t* src, int src_global) {
+__device__ __forceinline__ bool bq_push(const BlockQueue q, const uint32_t* src, int src_global) {
     const unsigned l = lane_id();
     int slot = -1;
     if (l == 0 && q.n() < BQ_RECORDS && bq_lock(q)) {
@@ -993,7 +993,7 @@ __device__ __noinline__ bool bq_push(const BlockQueue q, const uint32_t* src, in
 }
 
 // Pops the newest record into dst (shared memory, SW words); whole warp.
-__device__ __noinline__ bool bq_pop(const BlockQueue q, uint32_t* dst) {
+__device__ __forceinline__ bool bq_pop(const BlockQueue q, uint32_t* dst) {
     const unsigned l = lane_id();
     int slot = -1;
     if (l == 0 && q.n() > 0 && bq_lock(q)) {

@@ -95,8 +95,8 @@ __device__ __forceinline__ uint32_t rec_word(const uint32_t* src, int src_global
 
 // Enqueue one record of slot_words words copied from src.  Returns false when
 // the ring is full or the bounded retry loop gives up; the caller keeps the
-// record.  Out of line: it runs per handed-over task, not per branch node.
-static __device__ __noinline__ bool ring_push(Ring r, uint32_t slot_words, unsigned long long spin_limit, uint32_t test_stuck,
+// record.
+static __device__ __forceinline__ bool ring_push(Ring r, uint32_t slot_words, unsigned long long spin_limit, uint32_t test_stuck,
                                        Counters* ctr, const uint32_t* src, int src_global) {
     Pool* pool = r.ctl;
     const unsigned l = lane_id();
@@ -134,7 +134,7 @@ static __device__ __noinline__ bool ring_push(Ring r, uint32_t slot_words, unsig
 
 // Dequeue one record into dst (slot_words words).  Returns false if the ring
 // looks empty (a record still being published counts as empty).
-static __device__ __noinline__ bool ring_pop(Ring r, uint32_t slot_words, unsigned long long spin_limit, uint32_t* dst) {
+static __device__ __forceinline__ bool ring_pop(Ring r, uint32_t slot_words, unsigned long long spin_limit, uint32_t* dst) {
     Pool* pool = r.ctl;
     const unsigned l = lane_id();
     unsigned long long pos = 0;

@@ -10,7 +10,11 @@ Sources of truth, in order:
   * oracle.enumerate_csr: the restatement of the reference algorithm, for every
     case (count, hash and the number of generated tasks, which the device path
     must reproduce because it builds the same search tree).
-Usage: python tests/golden/make_golden.py [--datasets DIR] [--synthetic]
+Usage: python tests/golden/make_golden.py [--datasets DIR] [--synthetic] [--subsets]
+
+--subsets pins stated root ranges of the two full-size synthetic workloads,
+which hold too many maximal k-plexes for the oracle to enumerate whole: the
+roots of degeneracy rank r in [root_begin, root_end) (SUBSETS below).
 """
 import argparse
 import json
@@ -26,6 +30,14 @@ import kplex_b200 as kp  # noqa: E402
 import oracle  # noqa: E402
 
 README = {("soc-epinions.bin", 4, 30): 13172906, ("email-euall.bin", 3, 12): 32639016}
+
+# name -> (workload, root_begin, root_end): stated root ranges of the full-size
+# synthetic workloads that the oracle finishes in minutes
+SUBSETS = {
+    # email-shaped (k=3, q=12, truss on): 118 valid roots, two of them with more than
+    # 1024 local vertices (1028 and 1137)
+    "email:2560:2688": ("email", 2560, 2688),
+}
 
 
 def random_cases():
@@ -46,8 +58,24 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--datasets", default=os.path.join(ROOT, "datasets"))
     ap.add_argument("--synthetic", action="store_true", help="also run the full-size synthetic workloads (long)")
+    ap.add_argument("--subsets", action="store_true", help="pin the stated root ranges of the full-size workloads")
     args = ap.parse_args()
-    out = {"random": [], "workloads": {}, "datasets": {}}
+    dst = os.path.join(HERE, "golden.json")
+    if args.subsets:   # add (or refresh) the subset fixtures only
+        with open(dst) as f:
+            gold = json.load(f)
+        gold.setdefault("subsets", {})
+        for name, (wname, rb, re_) in SUBSETS.items():
+            w = kp.WORKLOADS[wname]
+            off, adj = kp.workload_graph(wname)
+            o = oracle.enumerate_csr(off, adj, w["k"], w["q"], w["truss"], root_begin=rb, root_end=re_)
+            gold["subsets"][name] = {"workload": wname, "root_begin": rb, "root_end": re_,
+                                     **{k: o[k] for k in ("count", "hash", "tasks", "valid_roots", "max_n", "max_left")}}
+            print(name, gold["subsets"][name], flush=True)
+        with open(dst, "w") as f:
+            json.dump(gold, f, indent=1, sort_keys=True)
+        return
+    out = {"random": [], "workloads": {}, "datasets": {}, "subsets": {}}
     for c in random_cases():
         off, adj = oracle.random_graph(c["n"], c["p"], c["seed"], [tuple(x) for x in c["planted"]])
         o = oracle.enumerate_csr(off, adj, c["k"], c["q"], c["truss"], threads=1)
@@ -75,13 +103,12 @@ def main():
             assert o["count"] == cnt, (fname, tr, o["count"], cnt)
             out["datasets"][f"{fname}:{k}:{q}:{tr}"] = {k2: o[k2] for k2 in ("count", "hash", "tasks", "valid_roots", "pn")}
     old = {}
-    dst = os.path.join(HERE, "golden.json")
     if os.path.exists(dst):
         with open(dst) as f:
             old = json.load(f)
-    for key in ("workloads", "datasets"):
+    for key in ("workloads", "datasets", "subsets", "reference_runs"):
         for name, rec in old.get(key, {}).items():
-            out[key].setdefault(name, rec)
+            out.setdefault(key, {}).setdefault(name, rec)
     with open(dst, "w") as f:
         json.dump(out, f, indent=1, sort_keys=True)
     print("wrote", dst)

@@ -113,15 +113,22 @@ def test_shipped_datasets(kp, key):
     assert (g["count"], g["hash"], g["tasks"]) == (gold["count"], gold["hash"], gold["tasks"])
 
 
-@pytest.mark.parametrize("name", ["epinions", "email"])
-def test_full_size_synthetic(kp, name):
-    gold = golden()["workloads"].get(name)
-    if gold is None:
-        pytest.skip("no oracle fixture for this workload")
-    w = kp.WORKLOADS[name]
-    off, adj = kp.workload_graph(name)
-    g = kp.enumerate_csr(off, adj, w["k"], w["q"], w["thres"], w["truss"])
-    assert (g["count"], g["hash"], g["tasks"]) == (gold["count"], gold["hash"], gold["tasks"])
+def _subset_keys():
+    return sorted(golden().get("subsets", {}))
+
+
+@pytest.mark.parametrize("key", _subset_keys())
+def test_synthetic_subsets(kp, key):
+    """Stated root ranges of the full-size synthetic workloads (configs 2 and 3), which
+    hold too many maximal k-plexes for the oracle to enumerate whole, against the
+    oracle's fixture for the same roots."""
+    s = golden()["subsets"][key]
+    w = kp.WORKLOADS[s["workload"]]
+    off, adj = kp.workload_graph(s["workload"])
+    g = kp.enumerate_csr(off, adj, w["k"], w["q"], w["thres"], w["truss"], root_begin=s["root_begin"],
+                         root_end=s["root_end"])
+    assert (g["count"], g["hash"], g["tasks"], g["valid_roots"]) == (s["count"], s["hash"], s["tasks"], s["valid_roots"])
+    assert g["max_local_n"] == s["max_n"]
 
 
 def test_repeat_and_reuse(kp):
