@@ -229,6 +229,44 @@ def run_reference(args, cfg, off, adj):
     print(json.dumps(line), flush=True)
 
 
+def run_subsets(device: int, steps: int = 3):
+    """Stated root ranges of the full-size synthetic workloads (the epinions-shaped and
+    email-shaped graphs hold too many maximal k-plexes to enumerate whole in a bench
+    step): device throughput on each, checked against the oracle's committed fixture
+    (tests/golden/golden.json "subsets")."""
+    import torch
+    with open(os.path.join(ROOT, "tests", "golden", "golden.json")) as f:
+        subsets = json.load(f).get("subsets", {})
+    out = {}
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{device}")
+    for key, s in sorted(subsets.items()):
+        w = kp.WORKLOADS[s["workload"]]
+        off, adj = kp.workload_graph(s["workload"])
+        prep = kp.prepare(off, adj, w["k"], w["q"], w["thres"], w["truss"], device=device,
+                          root_begin=s["root_begin"], root_end=s["root_end"])
+        prep.search()
+        res = []
+        for _ in range(steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            res.append(prep.search())
+        prep.release()
+        dev_ms = sum(r["ms_device"] for r in res)
+        t0 = time.perf_counter()
+        e = kp.enumerate_csr(off, adj, w["k"], w["q"], w["thres"], w["truss"], device=device,
+                             root_begin=s["root_begin"], root_end=s["root_end"])
+        e2e_ms = (time.perf_counter() - t0) * 1e3
+        r = res[-1]
+        out[key] = {"workload": f"{s['workload']}-shaped synthetic, roots of rank [{s['root_begin']}, {s['root_end']})",
+                    "value": r["count"] * steps / (dev_ms / 1e3), "unit": UNIT, "ms_per_step": dev_ms / steps,
+                    "count": r["count"], "hash": f"{r['hash']:#018x}",
+                    "exact_vs_oracle_fixture": (r["count"], r["hash"], r["tasks"]) == (s["count"], s["hash"], s["tasks"]),
+                    "max_local_n": r["max_local_n"], "nodes": r["nodes"],
+                    "e2e": {"value": e["count"] / (e2e_ms / 1e3), "unit": UNIT, "ms": e2e_ms},
+                    "bnb_bytes_per_ms": r["bnb_bytes"] / r["ms_bnb"] if r["ms_bnb"] else None}
+    return out
+
+
 def _pct(xs, p):
     xs = sorted(xs)
     if not xs:
@@ -396,6 +434,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-subsets", action="store_true",
+                    help="skip the pinned root ranges of the full-size synthetic workloads")
     ap.add_argument("--no-cudaplex", action="store_true",
                     help="skip the one run of the reference CudaPlex (oracle/_ref/cudaplex) on the same graph")
     ap.add_argument("--mode", default="plain", choices=["plain", "batched", "served"],
@@ -574,6 +614,8 @@ def main():
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_sample(off, adj, cfg, budget_s=args.cpu_budget)[0]
+    if rank == 0 and world == 1 and not args.no_subsets and shard_count == 0:
+        line["subsets"] = run_subsets(local)
     if rank == 0 and world == 1 and not args.no_cudaplex and shard_count == 0:
         ref = cudaplex_run(cfg)
         if ref is not None:

@@ -1063,15 +1063,15 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
         }
         if (have) {
             if (ww.stop - ww.sbot >= 2 && (ww.nodes() & 3) == 0) {   // donate the oldest stacked record
-                // to an idle warp of this block when there is one, else (every 64
+                // to an idle warp of this block when there is one, else (every 256
                 // nodes) to the global pool when it runs low.  The pool's head and
-                // tail share a line that idle warps poll with atomics: a busy warp
-                // that read them every 16 nodes lost 13% of the search to that line.
+                // tail share a line that idle warps poll with atomics: busy warps
+                // that read it every 16 nodes spent 15% of the search waiting on it.
                 int give = 0;
                 if (l == 0) {
                     const uint32_t iw = BQ.idle_warps();
                     if (iw > 0 && BQ.n() < iw) give = 1;
-                    else if ((ww.nodes() & 63) == 0 && pool_size(sp) < sp.low_water) give = 2;
+                    else if ((ww.nodes() & 255) == 0 && pool_size(sp) < sp.low_water) give = 2;
                 }
                 give = __shfl_sync(FULL, give, 0);
                 if (give) {
