@@ -59,8 +59,25 @@ def main():
     ap.add_argument("--datasets", default=os.path.join(ROOT, "datasets"))
     ap.add_argument("--synthetic", action="store_true", help="also run the full-size synthetic workloads (long)")
     ap.add_argument("--subsets", action="store_true", help="pin the stated root ranges of the full-size workloads")
+    ap.add_argument("--batch", action="store_true",
+                    help="pin the batched workload's original draws: the first 512 graphs of seed 4 without "
+                         "the k=4, q<12 ones (those hold up to hundreds of millions of plexes each)")
     args = ap.parse_args()
     dst = os.path.join(HERE, "golden.json")
+    if args.batch:
+        with open(dst) as f:
+            gold = json.load(f)
+        rows = []
+        for i, (off, adj, k, q) in enumerate(kp.batch_workload(512, 4)):
+            if k == 4 and q < 12:
+                continue
+            o = oracle.enumerate_csr(off, adj, k, q, 0)
+            rows.append([i, k, q, o["count"], o["hash"]])
+        gold["batch_original"] = {"seed": 4, "first": 512, "excluded": "k == 4 and q < 12", "graphs": rows}
+        with open(dst, "w") as f:
+            json.dump(gold, f, indent=1, sort_keys=True)
+        print("batch_original:", len(rows), "graphs,", sum(r[3] for r in rows), "plexes")
+        return
     if args.subsets:   # add (or refresh) the subset fixtures only
         with open(dst) as f:
             gold = json.load(f)

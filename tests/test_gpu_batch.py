@@ -65,3 +65,23 @@ def test_autotuned_schedule_same_results(kp):
     a, _ = kp.enumerate_batch(graphs)
     b, _ = kp.enumerate_batch(graphs, **tuned)
     assert [(r["count"], r["hash"]) for r in a] == [(r["count"], r["hash"]) for r in b]
+
+
+def test_batch_original_draws_vs_oracle_fixture(kp):
+    """The batched workload as drawn (no raised q): the first 512 graphs of seed 4
+    without the k=4, q<12 ones, in one launch, against the oracle's per-graph
+    fixture (tests/golden/golden.json "batch_original")."""
+    import json
+    import os
+    from conftest import GOLDEN
+    with open(os.path.join(GOLDEN, "golden.json")) as f:
+        fix = json.load(f).get("batch_original")
+    if fix is None:
+        pytest.skip("no batch_original fixture")
+    allg = kp.batch_workload(fix["first"], fix["seed"])
+    graphs = [allg[i] for i, *_ in fix["graphs"]]
+    per, tot = kp.enumerate_batch(graphs)
+    assert tot["status"] == 0
+    for (i, k, q, count, h), r, g in zip(fix["graphs"], per, graphs):
+        assert (g[2], g[3]) == (k, q)
+        assert (r["count"], r["hash"]) == (count, h), i
