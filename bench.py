@@ -281,7 +281,7 @@ def run_batched(args):
     import torch
     torch.cuda.set_device(0)
     graphs = kp.batch_workload(args.batch_count, 4, q_per_k=0 if args.batch_full else 4)
-    tuned, tune_ms = kp.autotune_batch(graphs, sample=min(128, len(graphs)))
+    tuned, tune_ms = kp.autotune_batch(graphs, sample=min(args.tune_sample, len(graphs)))
     prep = kp.prepare_batch(graphs, **tuned)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda:0")
     for _ in range(args.warmup):
@@ -303,12 +303,28 @@ def run_batched(args):
     t0 = time.perf_counter()
     per_e2e, tot_e2e = kp.enumerate_batch(graphs, **tuned)
     e2e_ms = (time.perf_counter() - t0) * 1e3
-    # one plain launch per graph, back to back
+    # one plain launch per graph, back to back (each timed, for the tail analysis)
+    seq, seq_each = [], []
     t0 = time.perf_counter()
-    seq = [kp.enumerate_csr(o, a, k, q) for (o, a, k, q) in graphs]
+    for (o, a, k, q) in graphs:
+        t1 = time.perf_counter()
+        seq.append(kp.enumerate_csr(o, a, k, q))
+        seq_each.append((time.perf_counter() - t1) * 1e3)
     seq_ms = (time.perf_counter() - t0) * 1e3
     exact = all((per[i]["count"], per[i]["hash"]) == (seq[i]["count"], seq[i]["hash"]) ==
                 (per_e2e[i]["count"], per_e2e[i]["hash"]) for i in range(len(graphs)))
+    # where the time goes: a batched launch cannot end before its largest graph does
+    order = sorted(range(len(graphs)), key=lambda i: -seq[i]["ms_device"])
+    tail = {"largest_graph": {"index": order[0], "count": seq[order[0]]["count"],
+                              "plain_device_ms": seq[order[0]]["ms_device"]},
+            "top10_share_of_plain_device_ms": sum(seq[i]["ms_device"] for i in order[:10]) /
+                                              max(1e-9, sum(r["ms_device"] for r in seq)),
+            "plain_device_ms_total": sum(r["ms_device"] for r in seq),
+            "plain_host_ms_total": seq_ms - sum(r["ms_device"] for r in seq),
+            "batched_device_ms": dev_ms / args.steps,
+            "batched_idle_warp_share": tot["idle_warp_ms"] / (tot["search_warps"] * tot["ms_bnb"])
+                                       if tot["search_warps"] and tot["ms_bnb"] else None}
+    orig = batch_original_subset(tuned)
     count = tot["count"]
     h2d = sum(4 * (len(o) + len(a)) for (o, a, _, _) in graphs)
     line = {"metric": METRIC + " (batched)", "value": count * args.steps / (dev_ms / 1e3), "unit": UNIT,
@@ -324,8 +340,35 @@ def run_batched(args):
             "sequential_plain": {"value": count / (seq_ms / 1e3), "unit": UNIT, "ms": seq_ms,
                                  "launches": len(graphs)},
             "batched_e2e_over_sequential": seq_ms / e2e_ms,
+            "tail": tail, "original_draws_subset": orig,
             "gpu_launches": sum(t["gpu_launches"] for _, t in res), "clocks": clocks}
-    print(json.dumps(line), flush=True)
+    return line
+
+
+def batch_original_subset(tuned):
+    """The batched workload as drawn (q not raised), on the stated subset the oracle
+    pins (tests/golden/golden.json "batch_original": the first 512 graphs of seed 4
+    without the k=4, q<12 ones): one batched call against one plain call per graph,
+    both end to end, and every graph's count and hash against the fixture."""
+    with open(os.path.join(ROOT, "tests", "golden", "golden.json")) as f:
+        fix = json.load(f).get("batch_original")
+    if fix is None:
+        return None
+    allg = kp.batch_workload(fix["first"], fix["seed"])
+    graphs = [allg[i] for i, *_ in fix["graphs"]]
+    kp.enumerate_batch(graphs, **tuned)   # warm the workspace for this shape
+    t0 = time.perf_counter()
+    per, tot = kp.enumerate_batch(graphs, **tuned)
+    b_ms = (time.perf_counter() - t0) * 1e3
+    t0 = time.perf_counter()
+    seq = [kp.enumerate_csr(o, a, k, q) for (o, a, k, q) in graphs]
+    s_ms = (time.perf_counter() - t0) * 1e3
+    exact = all((p["count"], p["hash"]) == (s["count"], s["hash"]) == (c, h)
+                for p, s, (_, _, _, c, h) in zip(per, seq, fix["graphs"]))
+    return {"workload": f"{len(graphs)} graphs: the first {fix['first']} of seed {fix['seed']} "
+                        f"without {fix['excluded']}, q as drawn", "count": tot["count"],
+            "batched_e2e_ms": b_ms, "sequential_plain_ms": s_ms, "batched_over_sequential": s_ms / b_ms,
+            "batched_device_ms": tot["ms_device"], "exact_vs_oracle_fixture": exact}
 
 
 def served_requests(rate: float, duration: float, seed: int = 5):
@@ -419,7 +462,7 @@ def run_served(args):
                     "h2d_bytes_per_step": sum(4 * (len(r[1]) + len(r[2])) for r in reqs),
                     "d2h_bytes_per_step": 88 * len(reqs)},
             "clocks": clocks}
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def main():
@@ -444,7 +487,12 @@ def main():
     ap.add_argument("--batch-count", type=int, default=4096)
     ap.add_argument("--batch-full", action="store_true",
                     help="batched: keep q < 4k (about 12 billion plexes, hours of GPU time)")
-    ap.add_argument("--rate", type=float, default=5.0, help="served: requests per second")
+    ap.add_argument("--rate", type=float, default=40.0,
+                    help="served: requests per second (40/s asks about 1.4 s of GPU work per second of one-at-a-time "
+                         "service, more than one request at a time can deliver)")
+    ap.add_argument("--tune-sample", type=int, default=128, help="batched: graphs the autotuner times")
+    ap.add_argument("--no-modes", action="store_true",
+                    help="plain: skip the batched and served records that the default run adds to its line")
     ap.add_argument("--duration", type=float, default=60.0, help="served: seconds of arrivals")
     ap.add_argument("--slots", type=int, default=2)
     ap.add_argument("--max-batch", type=int, default=256)
@@ -459,10 +507,10 @@ def main():
                     help="plain, one GPU: search only the roots of rank r % shards == 0 (a small case for profiling)")
     args = ap.parse_args()
     if args.mode == "batched" and args.impl == "ours":
-        run_batched(args)
+        print(json.dumps(run_batched(args)), flush=True)
         return
     if args.mode == "served" and args.impl == "ours":
-        run_served(args)
+        print(json.dumps(run_served(args)), flush=True)
         return
     if args.workload is None:
         args.workload = DEFAULT_WORKLOAD if os.path.exists(DEFAULT_WORKLOAD.split(":")[0]) else "small"
@@ -627,9 +675,19 @@ def main():
                                        "wall": ref["wall_ms"] / e2e_max if e2e_max > 0 else None,
                                        "ours_ms_ref_region": ours_ref,
                                        "count_equal": ref.get("count") == (total_count & 0xffffffff)}
+    prep.release()
+    if rank == 0 and world == 1 and not args.no_modes and shard_count == 0:
+        # the batched and served targets, measured in the same run (outside the timed steps)
+        import argparse as _ap
+        for key, fn, extra in (("batched", run_batched, dict(steps=2, warmup=1, tune_sample=64)),
+                               ("served", run_served, {})):
+            sub = _ap.Namespace(**{**vars(args), **extra})
+            try:
+                line[key] = fn(sub)
+            except Exception as exc:   # a failing sub-record must not cost the headline line
+                line[key] = {"error": f"{type(exc).__name__}: {exc}"[:300]}
     if rank == 0:
         print(json.dumps(line), flush=True)
-    prep.release()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
