@@ -37,6 +37,10 @@ SUBSETS = {
     # email-shaped (k=3, q=12, truss on): 118 valid roots, two of them with more than
     # 1024 local vertices (1028 and 1137)
     "email:2560:2688": ("email", 2560, 2688),
+    # epinions-shaped (k=4, q=30): two roots inside planted density-0.9 groups (local
+    # subgraphs of 56 and 50 vertices; 7.4 M and 0.44 M maximal 4-plexes)
+    "epinions:13158:13159": ("epinions", 13158, 13159),
+    "epinions:13590:13591": ("epinions", 13590, 13591),
 }
 
 
