@@ -322,8 +322,8 @@ def run_batched(args):
             "plain_device_ms_total": sum(r["ms_device"] for r in seq),
             "plain_host_ms_total": seq_ms - sum(r["ms_device"] for r in seq),
             "batched_device_ms": dev_ms / args.steps,
-            "batched_idle_warp_share": tot["idle_warp_ms"] / (tot["search_warps"] * tot["ms_bnb"])
-                                       if tot["search_warps"] and tot["ms_bnb"] else None}
+            "batched_warp_share": {x: tot[x + "_warp_ms"] / (tot["search_warps"] * tot["ms_bnb"])
+                                   if tot["search_warps"] and tot["ms_bnb"] else None for x in ("bnb", "ks", "idle")}}
     orig = batch_original_subset(tuned)
     count = tot["count"]
     h2d = sum(4 * (len(o) + len(a)) for (o, a, _, _) in graphs)
