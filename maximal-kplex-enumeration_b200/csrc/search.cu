@@ -1036,6 +1036,11 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
     if (l < 16) CT[l] = 0ull;
     if (l < STACK_CACHE) m.SCT()[l] = 0xffffffffu;
     __syncwarp();
+    // the warp's mbarrier for bulk copies into its shared memory (counter slot 15)
+    uint32_t tma_phase = 0;
+    bool tma_ok = true;
+    if (l == 0) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"((unsigned)__cvta_generic_to_shared(&CT[15])) : "memory");
+    __syncwarp();
     WarpWork ww{sp.stacks + (uint64_t)warp * sp.stack_depth * SW, 0ull, 0ull, CT};
     const unsigned long long resume_at = sp.pause_at / 2 > 0 ? sp.pause_at / 2 : 1;
     bool have = false, counted = false, ks_active = false, paused = false, is_idle = false;
@@ -1095,15 +1100,32 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
                 }
                 A = R.A;
                 same_root = 0;
-            } else if (++same_root == sp.stage_after && R.n * R.W <= sp.a_words) {
-                // the warp keeps working on this root: copy its adjacency rows to shared memory
-                const uint4* src = reinterpret_cast<const uint4*>(R.A);
-                uint4* dst = reinterpret_cast<uint4*>(m.A());
-                #pragma unroll 1
-                for (uint32_t i = l; i < R.n * R.W / 4; i += 32) dst[i] = __ldg(src + i);
+            } else if (++same_root == sp.stage_after && R.n * R.W <= sp.a_words && tma_ok) {
+                // the warp keeps working on this root: one bulk copy (global -> this CTA's shared
+                // memory, no multicast) of its adjacency rows, completion on the warp's mbarrier
+                const uint32_t bytes = R.n * R.W * 4;
+                const unsigned mb = (unsigned)__cvta_generic_to_shared(&CT[15]);
+                const unsigned dsts = (unsigned)__cvta_generic_to_shared(m.A());
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 __syncwarp();
-                A = m.A();
-                if (l == 0) ++CT[CT_STAGE];
+                if (l == 0) {
+                    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(mb), "r"(bytes) : "memory");
+                    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                                 :: "r"(dsts), "l"(R.A), "r"(bytes), "r"(mb) : "memory");
+                }
+                uint32_t done = 0;
+                for (int it = 0; it < (1 << 22) && !done; ++it)
+                    asm volatile("{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+                                 : "=r"(done) : "r"(mb), "r"(tma_phase) : "memory");
+                done = __all_sync(FULL, done);
+                if (done) {
+                    tma_phase ^= 1u;
+                    A = m.A();
+                    if (l == 0) ++CT[CT_STAGE];
+                } else {   // gave up: keep reading the arena, stage nothing more
+                    if (l == 0) raise_error(sp.ctr, KPLEX_ERR_TIMEOUT);
+                    tma_ok = false;
+                }
             }
             if (l == 0) ++ww.nodes();
             const long long b0 = clock64();

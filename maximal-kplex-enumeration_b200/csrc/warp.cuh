@@ -8,21 +8,11 @@ namespace kplex {
 
 constexpr unsigned FULL = 0xffffffffu;
 
-__device__ __forceinline__ int warp_sum(int v) {
-#pragma unroll
-    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
-    return v;
-}
-__device__ __forceinline__ unsigned warp_min(unsigned v) {
-#pragma unroll
-    for (int o = 16; o; o >>= 1) v = min(v, __shfl_xor_sync(FULL, v, o));
-    return v;
-}
-__device__ __forceinline__ unsigned warp_or(unsigned v) {
-#pragma unroll
-    for (int o = 16; o; o >>= 1) v |= __shfl_xor_sync(FULL, v, o);
-    return v;
-}
+// Warp reductions in one instruction each (the sm_80+ redux.sync unit); warp_sum
+// is used for counts, which are never negative.
+__device__ __forceinline__ int warp_sum(int v) { return (int)__reduce_add_sync(FULL, (unsigned)v); }
+__device__ __forceinline__ unsigned warp_min(unsigned v) { return __reduce_min_sync(FULL, v); }
+__device__ __forceinline__ unsigned warp_or(unsigned v) { return __reduce_or_sync(FULL, v); }
 // exclusive prefix sum across the warp; *total receives the sum
 __device__ __forceinline__ int warp_excl_scan(int v, int* total) {
     const unsigned l = lane_id();
