@@ -487,9 +487,9 @@ def main():
     ap.add_argument("--batch-count", type=int, default=4096)
     ap.add_argument("--batch-full", action="store_true",
                     help="batched: keep q < 4k (about 12 billion plexes, hours of GPU time)")
-    ap.add_argument("--rate", type=float, default=40.0,
-                    help="served: requests per second (40/s asks about 1.4 s of GPU work per second of one-at-a-time "
-                         "service, more than one request at a time can deliver)")
+    ap.add_argument("--rate", type=float, default=80.0,
+                    help="served: requests per second (one request at a time was busy 35.5 s of 60 s at 40/s, so "
+                         "80/s asks for more than it can deliver)")
     ap.add_argument("--tune-sample", type=int, default=128, help="batched: graphs the autotuner times")
     ap.add_argument("--no-modes", action="store_true",
                     help="plain: skip the batched and served records that the default run adds to its line")

@@ -147,6 +147,10 @@ extern "C" int kplex_search_noalloc(const uint32_t* d_off, const uint32_t* d_adj
     sp.root_begin = p->root_end ? p->root_begin : 0u;
     sp.root_end = p->root_end ? p->root_end : 0xffffffffu;
     sp.spin_limit = 1ull << 24;
+    if (p->flags & KPLEX_FLAG_TEST_NO_WAIT) {   // failure-detection test hook, as in kplex_enumerate_csr
+        sp.test_stuck = 1;
+        sp.spin_limit = 1u << 14;
+    }
     uint32_t launches = 0;
 
     NA_CK(cudaMemsetAsync(ctr, 0, sizeof(Counters), st));

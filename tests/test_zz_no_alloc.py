@@ -63,3 +63,21 @@ def test_noalloc_rejects_oversized_graph(kp):
     rc = fn(*[b.data_ptr() for b in bufs], 50_000_000, ctypes.byref(p), ctypes.byref(r))
     assert rc == kp.ERR_NOMEM
     assert b"64 MiB" in kp.lib().kplex_last_error()
+
+
+def test_noalloc_reports_leftover_work_as_timeout(kp, orc):
+    """With the test hook that makes every bounded device wait give up (one pool slot
+    is claimed and never published), the call must end with KPLEX_ERR_TIMEOUT, not
+    with a short count, and the next call on the same array must be exact."""
+    off, adj = orc.random_graph(80, 0.15, 3, [(20, 0.9), (18, 0.95), (16, 1.0)])
+    want = kp.enumerate_csr(off, adj, 3, 8)
+    pre, bufs = _device_inputs(kp, off, adj, 3, 8, 0)
+    fn = _noalloc(kp)
+    p = kp.make_params(3, 8, 0.25, 0, flags=kp.FLAG_QUIET | kp.FLAG_TEST_NO_WAIT)
+    r = kp.Result()
+    rc = fn(*[b.data_ptr() for b in bufs], pre["pn"], ctypes.byref(p), ctypes.byref(r))
+    assert rc == kp.ERR_TIMEOUT and r.status == kp.ERR_TIMEOUT
+    p = kp.make_params(3, 8)
+    r = kp.Result()
+    rc = fn(*[b.data_ptr() for b in bufs], pre["pn"], ctypes.byref(p), ctypes.byref(r))
+    assert rc == 0 and (r.count, r.hash, r.tasks) == (want["count"], want["hash"], want["tasks"])
