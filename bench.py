@@ -267,6 +267,29 @@ def run_subsets(device: int, steps: int = 3):
     return out
 
 
+def run_sharding(args, off, adj, cfg, device: int = 0):
+    """Load balance of the multi-GPU root partition, measured on one GPU: every
+    shard of S in {2, 4, 8} searched in turn (each with the whole device, as it
+    would have on its own GPU), for the r % S rule and for the cost-weighted
+    partition.  The slowest shard bounds an S-GPU run: balance = mean / max."""
+    out = {}
+    for mode in ("modulo", "weighted"):
+        flags = kp.FLAG_QUIET | (kp.FLAG_SHARD_WEIGHTED if mode == "weighted" else 0)
+        for S in (2, 4, 8):
+            ms, cnt = [], 0
+            for s in range(S):
+                prep = kp.prepare(off, adj, cfg["k"], cfg["q"], cfg["t"], cfg["truss"], flags=flags, device=device,
+                                  shard_index=s, shard_count=S)
+                prep.search()
+                r = prep.search()
+                prep.release()
+                ms.append(r["ms_device"])
+                cnt += r["count"]
+            out[f"{mode}_{S}"] = {"shard_ms": ms, "max_ms": max(ms), "balance": (sum(ms) / S) / max(ms),
+                                  "count": cnt}
+    return out
+
+
 def _pct(xs, p):
     xs = sorted(xs)
     if not xs:
@@ -499,6 +522,8 @@ def main():
     ap.add_argument("--no-split-grid", dest="split_grid", action="store_false",
                     help="served: give each launch the whole device instead of 1/slots of the SMs")
     ap.add_argument("--mem-budget", type=int, default=32, help="served: GiB")
+    ap.add_argument("--shard-mode", default="weighted", choices=["weighted", "modulo"],
+                    help="multi-GPU root partition: cost-weighted (kplex_partition_roots) or r % world")
     ap.add_argument("--blocks-per-sm", type=int, default=0,
                     help="plain: 8-warp blocks per SM of the search kernel (2 or 3; 0 = the library default)")
     ap.add_argument("--stage-after", type=int, default=0,
@@ -545,7 +570,10 @@ def main():
     sched = dict(blocks_per_sm=args.blocks_per_sm, stage_after=args.stage_after)
     if args.blocks_per_sm or args.stage_after:
         cfg["schedule"] = {k: v for k, v in sched.items() if v}
-    prep = kp.prepare(off, adj, cfg["k"], cfg["q"], cfg["t"], cfg["truss"], device=local,
+    shard_flags = kp.FLAG_QUIET | (kp.FLAG_SHARD_WEIGHTED if world > 1 and args.shard_mode == "weighted" else 0)
+    if world > 1:
+        cfg["shard_mode"] = args.shard_mode
+    prep = kp.prepare(off, adj, cfg["k"], cfg["q"], cfg["t"], cfg["truss"], flags=shard_flags, device=local,
                       shard_index=shard_index, shard_count=shard_count, **sched)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
     for _ in range(args.warmup):
@@ -581,7 +609,7 @@ def main():
     e2e_count = 0
     e2e_parts = {}
     for _ in range(args.e2e_steps):
-        r = kp.enumerate_csr(off, adj, cfg["k"], cfg["q"], cfg["t"], cfg["truss"], device=local,
+        r = kp.enumerate_csr(off, adj, cfg["k"], cfg["q"], cfg["t"], cfg["truss"], flags=shard_flags, device=local,
                              shard_index=shard_index, shard_count=shard_count, **sched)
         e2e_ms.append(r["ms_total"])
         e2e_ref.append(r["ms_ref_region"])
@@ -676,6 +704,11 @@ def main():
                                        "ours_ms_ref_region": ours_ref,
                                        "count_equal": ref.get("count") == (total_count & 0xffffffff)}
     prep.release()
+    if rank == 0 and world == 1 and not args.no_modes and shard_count == 0:
+        try:
+            line["sharding"] = run_sharding(args, off, adj, cfg, local)
+        except Exception as exc:
+            line["sharding"] = {"error": f"{type(exc).__name__}: {exc}"[:300]}
     if rank == 0 and world == 1 and not args.no_modes and shard_count == 0:
         # the batched and served targets, measured in the same run (outside the timed steps)
         import argparse as _ap

@@ -43,6 +43,9 @@ extern "C" {
                                          spillToHost/reFillTasks, host:168-251, but never calls them) */
 #define KPLEX_FLAG_TEST_NO_WAIT 0x8u  /* test hook: branch warps give up every bounded wait at once, so the
                                          run must end with KPLEX_ERR_TIMEOUT instead of hanging */
+#define KPLEX_FLAG_SHARD_WEIGHTED 0x10u /* with shard_count > 1: this call searches the roots that
+                                         kplex_partition_roots assigns to shard_index (cost-weighted)
+                                         instead of r % shard_count == shard_index */
 
 /* Run parameters: the reference's CLI flags (main.cu:31-53) plus device knobs. */
 typedef struct {
@@ -264,6 +267,16 @@ void kplex_server_destroy(kplex_server* s);
  * *best_ms receives the winner's device time on the sample. */
 int kplex_autotune_batch(const kplex_job* jobs, uint32_t njobs, const kplex_params* common, uint32_t sample,
                          kplex_params* best, double* best_ms);
+
+/* Cost-weighted partition of the roots over `shards` processes (no reference
+ * counterpart; the reference runs on one GPU).  Input: the pruned graph and
+ * degeneracy order from kplex_preprocess_csr.  owner_out[r] (one byte per root
+ * rank r < pn - q + 2) receives the shard that searches root r: roots are taken
+ * largest estimated cost first ((later neighbours + 1)^2) and given to the least
+ * loaded shard, so every process computes the same assignment.  Returns the
+ * number of roots, or -status.  KPLEX_FLAG_SHARD_WEIGHTED makes a search use it. */
+long long kplex_partition_roots(const uint32_t* offsets, const uint32_t* neighbors, const int32_t* dpos,
+                                const int32_t* dseq, uint32_t pn, int q, uint32_t shards, uint8_t* owner_out);
 
 const char* kplex_status_string(int status);
 /* Text of the last failure on the calling thread (CUDA message, parse error, ...). */

@@ -107,7 +107,9 @@ __global__ void __launch_bounds__(256) decompose_kernel(SearchParams sp) {
         desc.graph = g;
         desc.k = k;
         desc.q = q;
-        if ((sp.shard_count > 1 && r % sp.shard_count != sp.shard_index) ||   // another GPU's root
+        const bool other = sp.root_owner ? sp.root_owner[r] != sp.shard_index
+                                         : (sp.shard_count > 1 && r % sp.shard_count != sp.shard_index);
+        if (other ||   // another GPU's root
             r - gi.root_base < sp.root_begin || r - gi.root_base >= sp.root_end) {   // outside the stated range
             if (l == 0) sp.roots[r] = desc;
             __syncwarp();

@@ -153,6 +153,7 @@ struct SearchParams {
     uint32_t hash_on;
     uint32_t shard_index, shard_count;
     uint32_t root_begin, root_end;   // roots of rank r outside [root_begin, root_end) are skipped
+    const uint8_t* root_owner;       // cost-weighted shards: root r is searched iff root_owner[r] == shard_index
     uint32_t test_stuck;       // test hook: the first push claims a slot and never publishes it
     const GraphInfo* graphs;   // ngraphs entries
     uint32_t ngraphs;

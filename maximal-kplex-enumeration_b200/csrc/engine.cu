@@ -150,7 +150,8 @@ void free_prepared(kplex_prepared* h) {
     if (!h) return;
     cudaSetDevice(h->device);
     delete h->replay;
-    void* ps[9] = {h->d_off, h->d_adj, h->d_dpos, h->d_dseq, h->d_orig, h->d_graphs, h->d_gcount, h->d_ghash, h->d_gvalid};
+    void* ps[10] = {h->d_off, h->d_adj, h->d_dpos, h->d_dseq, h->d_orig, h->d_graphs, h->d_gcount, h->d_ghash, h->d_gvalid,
+                    h->d_owner};
     for (void* x : ps) if (x) cudaFreeAsync(x, h->stream);
     delete h;
 }
@@ -240,6 +241,17 @@ int prepare_set(const std::vector<HostJob>& jobs, const kplex_params* p, Workspa
     CK(cudaMemcpyAsync(h->d_dseq, dseq.data(), dseq.size() * 4, cudaMemcpyHostToDevice, d->stream));
     CK(cudaMemcpyAsync(h->d_orig, orig.data(), orig.size() * 4, cudaMemcpyHostToDevice, d->stream));
     CK(cudaMemcpyAsync(h->d_graphs, h->ginfo.data(), G * sizeof(GraphInfo), cudaMemcpyHostToDevice, d->stream));
+    std::vector<uint8_t> owner;
+    if ((p->flags & KPLEX_FLAG_SHARD_WEIGHTED) && p->shard_count > 1) {
+        // cost-weighted shards: every graph's roots, each graph partitioned on its own
+        if (p->shard_count > 255) { g_last_error = "at most 255 weighted shards"; return fail(KPLEX_ERR_PARAM); }
+        owner.assign(std::max<uint64_t>(R, 1), 0);
+        for (size_t g = 0; g < G; ++g)
+            weighted_root_owners(pres[g].g, pres[g].dpos, pres[g].dseq, h->ginfo[g].nroots, p->shard_count,
+                                 owner.data() + h->ginfo[g].root_base);
+        if (!dm(&h->d_owner, owner.size())) { cudaGetLastError(); g_last_error = "cudaMalloc for the root owners failed"; return fail(KPLEX_ERR_NOMEM); }
+        CK(cudaMemcpyAsync(h->d_owner, owner.data(), owner.size(), cudaMemcpyHostToDevice, d->stream));
+    }
     CK(cudaStreamSynchronize(d->stream));
     if (out) { out->pn = h->pn; out->pm = h->pm; out->ms_preprocess = ms_pre; }
     *out_h = h;
@@ -426,6 +438,7 @@ int search_impl(kplex_prepared* h, Workspace* d, kplex_result* out, kplex_result
     sp.shard_count = P.shard_count > 1 ? P.shard_count : 1u;
     sp.root_begin = P.root_end ? P.root_begin : 0u;
     sp.root_end = P.root_end ? P.root_end : 0xffffffffu;
+    sp.root_owner = h->d_owner;
     sp.spin_limit = 1ull << 24;
 
     if ((rc = d->ctr.ensure(sizeof(Counters)))) return rc;
@@ -630,6 +643,21 @@ long long kplex_preprocess_csr(const uint32_t* offsets, const uint32_t* neighbor
     }
     *out_m = pre.g.adj.size();
     return pn;
+}
+
+long long kplex_partition_roots(const uint32_t* offsets, const uint32_t* neighbors, const int32_t* dpos,
+                                const int32_t* dseq, uint32_t pn, int q, uint32_t shards, uint8_t* owner_out) {
+    if (!offsets || (!neighbors && offsets[pn]) || (pn && (!dpos || !dseq)) || !owner_out || shards == 0 || shards > 255)
+        return -KPLEX_ERR_PARAM;
+    Csr g;
+    g.n = pn;
+    g.off.assign(offsets, offsets + pn + 1);
+    g.adj.assign(neighbors, neighbors + offsets[pn]);
+    std::vector<int32_t> dp(dpos, dpos + pn), ds(dseq, dseq + pn);
+    const long long lim = (long long)pn - (long long)q + 2;   // src:44-45
+    const uint32_t nroots = lim > 0 ? (uint32_t)std::min<long long>(lim, pn) : 0u;
+    weighted_root_owners(g, dp, ds, nroots, shards, owner_out);
+    return nroots;
 }
 
 const char* kplex_status_string(int s) {

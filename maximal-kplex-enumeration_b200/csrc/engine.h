@@ -143,6 +143,7 @@ struct kplex_prepared {
     unsigned long long* d_gcount = nullptr;
     unsigned long long* d_ghash = nullptr;
     unsigned int* d_gvalid = nullptr;
+    uint8_t* d_owner = nullptr;      // cost-weighted shard of each root (KPLEX_FLAG_SHARD_WEIGHTED)
     kplex::Replay* replay = nullptr;  // the captured form of this set's search, once it has run
 };
 

@@ -190,3 +190,34 @@ int preprocess(const Csr& in, int k, int q, int truss, int threads, Prepped& out
 }
 
 }  // namespace kplex
+
+namespace kplex {
+
+// Cost-weighted partition of the root ranks [0, nroots) over `shards` owners, for
+// multi-GPU runs.  A root's work grows with its local subgraph, whose first layer
+// is the root's later neighbours (C1 is drawn from them, at most 1023 of them are
+// kept, src:87-131); the cost estimate is (later + 1)^2.  Roots are handed out
+// largest first to the least loaded owner (longest-processing-time rule), ties to
+// the smaller rank and the smaller owner, so every process computes the same
+// assignment from the same pruned graph.
+void weighted_root_owners(const Csr& g, const std::vector<int32_t>& dpos, const std::vector<int32_t>& dseq,
+                          uint32_t nroots, uint32_t shards, uint8_t* owner) {
+    std::vector<std::pair<uint64_t, uint32_t>> cost(nroots);
+    for (uint32_t r = 0; r < nroots; ++r) {
+        const uint32_t v = (uint32_t)dseq[r];
+        uint64_t later = 0;
+        for (uint32_t e = g.off[v]; e < g.off[v + 1]; ++e) later += dpos[g.adj[e]] > dpos[v];
+        later = std::min<uint64_t>(later, 1023);
+        cost[r] = {(later + 1) * (later + 1), r};
+    }
+    std::stable_sort(cost.begin(), cost.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+    std::vector<uint64_t> load(shards, 0);
+    for (const auto& c : cost) {
+        uint32_t best = 0;
+        for (uint32_t s = 1; s < shards; ++s) if (load[s] < load[best]) best = s;
+        load[best] += c.first;
+        owner[c.second] = (uint8_t)best;
+    }
+}
+
+}  // namespace kplex

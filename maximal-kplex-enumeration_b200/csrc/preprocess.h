@@ -9,4 +9,6 @@ struct Prepped {
     std::vector<uint32_t> orig;  // pruned id -> id in the input graph
 };
 int preprocess(const Csr& in, int k, int q, int truss, int threads, Prepped& out);
+void weighted_root_owners(const Csr& g, const std::vector<int32_t>& dpos, const std::vector<int32_t>& dseq,
+                          uint32_t nroots, uint32_t shards, uint8_t* owner);
 }  // namespace kplex

@@ -1052,6 +1052,7 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
         spins = 0;
     };
     Node<NW> t{};
+    unsigned long long next_pool = 0;   // node count at which this warp next reads the pool's size
     uint32_t cur_root = 0xffffffffu;
     RootView R{};
     Emitted<NW> e{};
@@ -1068,17 +1069,25 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
         }
         if (have) {
             if (ww.stop - ww.sbot >= 2 && (ww.nodes() & 3) == 0) {   // donate the oldest stacked record
-                // to an idle warp of this block when there is one, else (every 256
-                // nodes) to the global pool when it runs low.  The pool's head and
-                // tail share a line that idle warps poll with atomics: busy warps
-                // that read it every 16 nodes spent 15% of the search waiting on it.
-                int give = 0;
+                // to an idle warp of this block when there is one, else to the global
+                // pool when it runs low.  The pool's head and tail share a line that
+                // warps taking records hit with atomics: busy warps that read it every
+                // 16 nodes spent 15% of the search waiting on it.  So a warp reads it
+                // every 256 nodes while the pool holds enough, and every 16 while it
+                // runs low (then the line is mostly read, and spreading work fast
+                // matters: the end of a search, or many small graphs).
+                int give = 0, low = -1;
                 if (l == 0) {
                     const uint32_t iw = BQ.idle_warps();
                     if (iw > 0 && BQ.n() < iw) give = 1;
-                    else if ((ww.nodes() & 255) == 0 && pool_size(sp) < sp.low_water) give = 2;
+                    else if (ww.nodes() >= next_pool) {
+                        low = pool_size(sp) < sp.low_water;
+                        if (low) give = 2;
+                    }
                 }
                 give = __shfl_sync(FULL, give, 0);
+                low = __shfl_sync(FULL, low, 0);
+                if (low >= 0) next_pool = ww.nodes() + (low ? 16u : 256u);
                 if (give) {
                     const uint32_t* src = ww.stack + (ww.sbot % sp.stack_depth) * SW;
                     // the record becomes a unit of work before it can be seen (and taken)

@@ -19,7 +19,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libkplex.so")
 
 OK, ERR_PARAM, ERR_IO, ERR_FORMAT, ERR_CUDA, ERR_NOMEM, ERR_CAPACITY, ERR_TIMEOUT, ERR_NO_DEVICE, ERR_INTERNAL = range(10)
-FLAG_QUIET, FLAG_NO_HASH, FLAG_SPILL_HOST, FLAG_TEST_NO_WAIT = 0x1, 0x2, 0x4, 0x8
+FLAG_QUIET, FLAG_NO_HASH, FLAG_SPILL_HOST, FLAG_TEST_NO_WAIT, FLAG_SHARD_WEIGHTED = 0x1, 0x2, 0x4, 0x8, 0x10
 
 
 class KplexError(RuntimeError):
@@ -137,6 +137,9 @@ def lib() -> ctypes.CDLL:
                                            ctypes.c_int, ctypes.c_uint32, u32p, u32p, i32p, i32p, u32p,
                                            ctypes.POINTER(ctypes.c_uint64)]
         L.kplex_preprocess_csr.restype = ctypes.c_longlong
+        L.kplex_partition_roots.argtypes = [u32p, u32p, i32p, i32p, ctypes.c_uint32, ctypes.c_int, ctypes.c_uint32,
+                                            ctypes.POINTER(ctypes.c_uint8)]
+        L.kplex_partition_roots.restype = ctypes.c_longlong
         L.kplex_enumerate_batch.argtypes = [ctypes.POINTER(Job), ctypes.c_uint32, ctypes.POINTER(Params),
                                             ctypes.POINTER(Result), ctypes.POINTER(Result)]
         L.kplex_prepare_batch.argtypes = [ctypes.POINTER(Job), ctypes.c_uint32, ctypes.POINTER(Params),
@@ -297,6 +300,22 @@ def preprocess(off: np.ndarray, adj: np.ndarray, k: int, q: int, truss: int = 0,
         raise _err(int(-pn))
     return {"pn": int(pn), "off": o_off[: pn + 1], "adj": o_adj[: m.value], "dpos": o_dpos[:pn], "dseq": o_dseq[:pn],
             "orig": o_orig[:pn]}
+
+
+def partition_roots(pre: dict, q: int, shards: int) -> np.ndarray:
+    """Cost-weighted shard of every root (kplex_partition_roots) for a preprocess() result."""
+    i32 = ctypes.POINTER(ctypes.c_int32)
+    nroots = max(0, pre["pn"] - q + 2)
+    owner = np.zeros(max(nroots, 1), dtype=np.uint8)
+    off = np.ascontiguousarray(pre["off"], dtype=np.uint32)
+    adj = np.ascontiguousarray(pre["adj"] if len(pre["adj"]) else np.zeros(1, np.uint32), dtype=np.uint32)
+    dpos = np.ascontiguousarray(pre["dpos"], dtype=np.int32)
+    dseq = np.ascontiguousarray(pre["dseq"], dtype=np.int32)
+    rc = lib().kplex_partition_roots(_u32p(off), _u32p(adj), dpos.ctypes.data_as(i32), dseq.ctypes.data_as(i32),
+                                     pre["pn"], q, shards, owner.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)))
+    if rc < 0:
+        raise _err(int(-rc))
+    return owner[:nroots]
 
 
 def _batch_draws(count: int, seed: int, q_per_k: int = 0):

@@ -51,6 +51,9 @@ def lib() -> ctypes.CDLL:
                                                   ctypes.c_int, ctypes.POINTER(OracleResult)]
         L.oracle_enumerate_shard.argtypes = [u32p, u32p, ctypes.c_uint32, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                              ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(OracleResult)]
+        L.oracle_enumerate_owned.argtypes = [u32p, u32p, ctypes.c_uint32, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                             ctypes.c_int, ctypes.POINTER(ctypes.c_uint8), ctypes.c_uint64,
+                                             ctypes.c_uint32, ctypes.POINTER(OracleResult)]
         _lib = L
     return _lib
 
@@ -92,6 +95,19 @@ def enumerate_shard(off, adj, k: int, q: int, truss: int, shard_index: int, shar
     adj, pa = _u32(adj)
     r = OracleResult()
     rc = lib().oracle_enumerate_shard(po, pa, len(off) - 1, k, q, truss, threads, shard_index, shard_count, ctypes.byref(r))
+    if rc:
+        raise RuntimeError(f"oracle failed with {rc}")
+    return r.as_dict()
+
+
+def enumerate_owned(off, adj, k: int, q: int, truss: int, owner, me: int, threads: int = 0) -> dict:
+    """The roots r with owner[r] == me (an explicit partition of the degeneracy ranks)."""
+    off, po = _u32(off)
+    adj, pa = _u32(adj)
+    owner = np.ascontiguousarray(owner, dtype=np.uint8)
+    r = OracleResult()
+    rc = lib().oracle_enumerate_owned(po, pa, len(off) - 1, k, q, truss, threads,
+                                      owner.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), len(owner), me, ctypes.byref(r))
     if rc:
         raise RuntimeError(f"oracle failed with {rc}")
     return r.as_dict()

@@ -745,7 +745,8 @@ static void preprocess(const Graph& g0, const Params& P, Graph& pg, std::vector<
 }
 
 static Result run(const Graph& g0, const Params& P, int threads, uint64_t root_begin, uint64_t root_end,
-                  uint32_t shard_index = 0, uint32_t shard_count = 1, bool sequential_ksearch = false) {
+                  uint32_t shard_index = 0, uint32_t shard_count = 1, bool sequential_ksearch = false,
+                  const uint8_t* owner = nullptr, uint64_t nowner = 0) {
     Result R;
     auto t0 = std::chrono::steady_clock::now();
     Graph pg; std::vector<int> dpos, dseq; std::vector<uint32_t> orig;
@@ -773,7 +774,7 @@ static Result run(const Graph& g0, const Params& P, int threads, uint64_t root_b
 #pragma omp single
     {
         for (uint64_t ri = rb; ri < re; ++ri) {
-            if (shard_count > 1 && ri % shard_count != shard_index) continue;
+            if (owner ? (ri >= nowner || owner[ri] != shard_index) : (shard_count > 1 && ri % shard_count != shard_index)) continue;
 #pragma omp task firstprivate(ri, PG, DP, DS, OR, ST, PP, TC, TH, TT, OUT, seq, max_out)
             {
                 std::shared_ptr<Sub> sub = std::make_shared<Sub>();
@@ -872,6 +873,19 @@ int oracle_enumerate_shard(const uint32_t* off, const uint32_t* adj, uint32_t n,
     oracle::Graph g = oracle::from_csr(off, adj, n);
     oracle::Params P{k, q, truss};
     oracle::Result R = oracle::run(g, P, threads, 0, UINT64_MAX, shard_index, shard_count);
+    *out = oracle_result{R.count, R.hash, R.tasks, R.valid, R.truncated, R.depth_cap, R.too_big,
+                         R.pn, R.pm, R.max_n, R.max_left, R.ms_pre, R.ms_search};
+    return 0;
+}
+
+// The roots r (degeneracy rank) with owner[r] == me, for an explicit partition of
+// the roots (the device's cost-weighted shards).
+int oracle_enumerate_owned(const uint32_t* off, const uint32_t* adj, uint32_t n, int k, int q, int truss,
+                           int threads, const uint8_t* owner, uint64_t nowner, uint32_t me, oracle_result* out) {
+    if (k < 2 || q < 1 || !owner) return 1;
+    oracle::Graph g = oracle::from_csr(off, adj, n);
+    oracle::Params P{k, q, truss};
+    oracle::Result R = oracle::run(g, P, threads, 0, UINT64_MAX, me, 2, false, owner, nowner);
     *out = oracle_result{R.count, R.hash, R.tasks, R.valid, R.truncated, R.depth_cap, R.too_big,
                          R.pn, R.pm, R.max_n, R.max_left, R.ms_pre, R.ms_search};
     return 0;

@@ -40,6 +40,25 @@ def test_root_shards_sum_to_whole(kp, orc, shards):
     assert (tot_c, tot_h, tot_v) == (full["count"], full["hash"], full["valid_roots"])
 
 
+@pytest.mark.parametrize("shards", [2, 3])
+def test_weighted_shards_sum_to_whole(kp, orc, shards):
+    """Cost-weighted shards (KPLEX_FLAG_SHARD_WEIGHTED): each shard searches the roots
+    kplex_partition_roots gives it; the shards add up to the whole run and each
+    equals the oracle on the same roots."""
+    off, adj = kp.workload_graph("small")
+    full = kp.enumerate_csr(off, adj, 2, 8)
+    owner = kp.partition_roots(kp.preprocess(off, adj, 2, 8, 0), 8, shards)
+    tot_c = tot_h = 0
+    for s in range(shards):
+        g = kp.enumerate_csr(off, adj, 2, 8, flags=kp.FLAG_QUIET | kp.FLAG_SHARD_WEIGHTED, shard_index=s,
+                             shard_count=shards)
+        o = orc.enumerate_owned(off, adj, 2, 8, 0, owner, s, threads=4)
+        assert (g["count"], g["hash"], g["tasks"]) == (o["count"], o["hash"], o["tasks"])
+        tot_c += g["count"]
+        tot_h = (tot_h + g["hash"]) % (1 << 64)
+    assert (tot_c, tot_h) == (full["count"], full["hash"])
+
+
 def test_bounded_wait_reports_timeout(kp, orc):
     """Branch warps that give up every wait at once leave records behind: the call
     returns KPLEX_ERR_TIMEOUT instead of hanging, and the device stays usable."""
