@@ -1052,7 +1052,6 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
         spins = 0;
     };
     Node<NW> t{};
-    unsigned long long next_pool = 0;   // node count at which this warp next reads the pool's size
     uint32_t cur_root = 0xffffffffu;
     RootView R{};
     Emitted<NW> e{};
@@ -1069,25 +1068,19 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
         }
         if (have) {
             if (ww.stop - ww.sbot >= 2 && (ww.nodes() & 3) == 0) {   // donate the oldest stacked record
-                // to an idle warp of this block when there is one, else to the global
-                // pool when it runs low.  The pool's head and tail share a line that
-                // warps taking records hit with atomics: busy warps that read it every
-                // 16 nodes spent 15% of the search waiting on it.  So a warp reads it
-                // every 256 nodes while the pool holds enough, and every 16 while it
-                // runs low (then the line is mostly read, and spreading work fast
-                // matters: the end of a search, or many small graphs).
-                int give = 0, low = -1;
+                // to an idle warp of this block when there is one, else (every 256
+                // nodes) to the global pool when it runs low.  The pool's head and
+                // tail share a line that warps taking records hit with atomics: busy
+                // warps that read it every 16 nodes spent 15% of the search waiting
+                // on it (and reading it every 16 nodes only while it runs low cost
+                // 18%: on soc-epinions it runs low nearly all the time).
+                int give = 0;
                 if (l == 0) {
                     const uint32_t iw = BQ.idle_warps();
                     if (iw > 0 && BQ.n() < iw) give = 1;
-                    else if (ww.nodes() >= next_pool) {
-                        low = pool_size(sp) < sp.low_water;
-                        if (low) give = 2;
-                    }
+                    else if ((ww.nodes() & 255) == 0 && pool_size(sp) < sp.low_water) give = 2;
                 }
                 give = __shfl_sync(FULL, give, 0);
-                low = __shfl_sync(FULL, low, 0);
-                if (low >= 0) next_pool = ww.nodes() + (low ? 16u : 256u);
                 if (give) {
                     const uint32_t* src = ww.stack + (ww.sbot % sp.stack_depth) * SW;
                     // the record becomes a unit of work before it can be seen (and taken)
@@ -1259,11 +1252,30 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
             which = __shfl_sync(FULL, which, 0);
             if (which) {
                 const bool got = which == 1 ? pool_pop(sp, m.rec()) : ring_pop(sp, spill_ring(sp), m.rec());
-                if (l == 0) atomicExch(BQ.poller(), 0);
                 if (got) {
                     wake();
                     if (which == 2 && l == 0) ++CT[CT_REFILL];
                     load_record<NW>(m.rec(), Wt, &t, false);
+                    __syncwarp();
+                    // while holding the poller token, fetch a record for each other idle warp of the
+                    // block into the block queue (each record keeps its unit of work): with many small
+                    // tasks one poller per block otherwise leaves its block-mates waiting
+                    if (which == 1) {
+#pragma unroll 1
+                        for (int extra = 0; extra < 4; ++extra) {
+                            int more = 0;
+                            if (l == 0) more = BQ.idle_warps() > BQ.n() && BQ.n() < BQ_RECORDS && pool_size(sp) > 0;
+                            if (!__shfl_sync(FULL, more, 0)) break;
+                            if (!pool_pop(sp, m.rec())) break;
+                            if (!bq_push(BQ, m.rec(), 0)) {   // no room after all: hand it back to the pool
+                                if (!pool_push(sp, m.rec(), 0) && l == 0) raise_error(sp.ctr, KPLEX_ERR_INTERNAL);
+                                break;
+                            }
+                        }
+                    }
+                }
+                if (l == 0) atomicExch(BQ.poller(), 0);
+                if (got) {
                     have = true;
                     counted = true;
                     if (l == 0) atomicAdd(&sp.ctr->holders, 1u);
