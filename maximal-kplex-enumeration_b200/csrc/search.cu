@@ -1252,30 +1252,11 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
             which = __shfl_sync(FULL, which, 0);
             if (which) {
                 const bool got = which == 1 ? pool_pop(sp, m.rec()) : ring_pop(sp, spill_ring(sp), m.rec());
+                if (l == 0) atomicExch(BQ.poller(), 0);
                 if (got) {
                     wake();
                     if (which == 2 && l == 0) ++CT[CT_REFILL];
                     load_record<NW>(m.rec(), Wt, &t, false);
-                    __syncwarp();
-                    // while holding the poller token, fetch a record for each other idle warp of the
-                    // block into the block queue (each record keeps its unit of work): with many small
-                    // tasks one poller per block otherwise leaves its block-mates waiting
-                    if (which == 1) {
-#pragma unroll 1
-                        for (int extra = 0; extra < 4; ++extra) {
-                            int more = 0;
-                            if (l == 0) more = BQ.idle_warps() > BQ.n() && BQ.n() < BQ_RECORDS && pool_size(sp) > 0;
-                            if (!__shfl_sync(FULL, more, 0)) break;
-                            if (!pool_pop(sp, m.rec())) break;
-                            if (!bq_push(BQ, m.rec(), 0)) {   // no room after all: hand it back to the pool
-                                if (!pool_push(sp, m.rec(), 0) && l == 0) raise_error(sp.ctr, KPLEX_ERR_INTERNAL);
-                                break;
-                            }
-                        }
-                    }
-                }
-                if (l == 0) atomicExch(BQ.poller(), 0);
-                if (got) {
                     have = true;
                     counted = true;
                     if (l == 0) atomicAdd(&sp.ctr->holders, 1u);
