@@ -147,7 +147,7 @@ struct SearchParams {
     uint64_t scratch_words;    // words per warp
     uint32_t* ks_slots;        // k-search per-warp state (KS_WORDS each), kept across pauses
     uint32_t* stacks;          // branch stacks: warps * stack_depth * slot_words
-    uint32_t stack_depth;
+    uint32_t stack_depth;      // records per warp stack, a power of two
     uint32_t nwarps;           // branch warps launched
     uint32_t low_water;        // a branch warp donates work when the pool holds fewer records
     uint32_t hash_on;

@@ -499,7 +499,9 @@ int search_impl(kplex_prepared* h, Workspace* d, kplex_result* out, kplex_result
     sp.slot_words = 4 + 3 * Wt;
 
     // ---------------- pool, k-search slots, branch stacks
-    const unsigned long long cap = P.pool_slots ? P.pool_slots : 4194304ull;   // MAX_CAP, inc/common.h:10
+    // MAX_CAP (inc/common.h:10) by default; a ring's capacity is a power of two
+    unsigned long long cap = 4;
+    while (cap < (P.pool_slots ? P.pool_slots : 4194304ull)) cap *= 2;
     if ((rc = d->pool.ensure(sizeof(Pool)))) return rc;
     if ((rc = d->pool_seq.ensure((size_t)cap * 4))) return rc;
     if ((rc = d->pool_data.ensure((size_t)cap * sp.slot_words * 4))) return rc;
@@ -533,7 +535,8 @@ int search_impl(kplex_prepared* h, Workspace* d, kplex_result* out, kplex_result
     const uint32_t blocks = std::max<uint32_t>(1u, (uint32_t)d->sms * (uint32_t)per_sm / std::max<uint32_t>(grid_div, 1u));
     const uint32_t nwarps = blocks * warps_per_block;
     sp.nwarps = nwarps;
-    sp.stack_depth = nmax + 2;
+    sp.stack_depth = 4;   // a power of two of at least nmax + 2 (DFS depth is bounded by |C| <= n)
+    while (sp.stack_depth < nmax + 2) sp.stack_depth *= 2;
     sp.low_water = nwarps;
     // the reference pauses at MAX_CAP * thres - WARPS (src:2083, 2384): one record of slack per producer
     const long long pause = (long long)std::floor((double)cap * (double)P.thres) - (long long)blocks;

@@ -195,7 +195,8 @@ extern "C" int kplex_search_noalloc(const uint32_t* d_off, const uint32_t* d_adj
     int per_sm = 0;
     NA_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, warps_per_block * 32, smem_bytes));
     uint32_t blocks = (uint32_t)sms * (uint32_t)std::max(per_sm, 1);
-    sp.stack_depth = nmax + 2;
+    sp.stack_depth = 4;   // a power of two of at least nmax + 2
+    while (sp.stack_depth < nmax + 2) sp.stack_depth *= 2;
     const size_t stack_per_warp = (size_t)sp.stack_depth * sp.slot_words * 4;
     const size_t rec_bytes = (size_t)sp.slot_words * 4 + 4;
     const size_t min_slots = 4096;
@@ -207,7 +208,9 @@ extern "C" int kplex_search_noalloc(const uint32_t* d_off, const uint32_t* d_adj
     }
     sp.stacks = reinterpret_cast<uint32_t*>(base + o2);
     o2 = align_up(o2 + stacks_bytes, 256);
-    const unsigned long long cap = std::min<unsigned long long>((NOALLOC_BYTES - o2 - 512) / rec_bytes, 1ull << 20);
+    const unsigned long long fit = std::min<unsigned long long>((NOALLOC_BYTES - o2 - 512) / rec_bytes, 1ull << 20);
+    unsigned long long cap = 1;   // a ring's capacity is a power of two
+    while (cap * 2 <= fit) cap *= 2;
     sp.pool = pool;
     sp.pool_seq = reinterpret_cast<uint32_t*>(base + o2);
     o2 = align_up(o2 + (size_t)cap * 4, 256);

@@ -688,10 +688,12 @@ struct Node {
 enum : int { CT_CNT, CT_HSUM, CT_TASKS, CT_NODES, CT_BB, CT_TOT_CNT, CT_TOT_HSUM, CT_STAGE, CT_KS_CYC, CT_SPILL,
              CT_REFILL, CT_BNB_CYC, CT_IDLE_CYC, CT_KS_TASKS };
 // A warp's depth-first stack (records [sbot, stop) of `stack`, a ring of
-// stack_depth records) and its counters in shared memory.
+// stack_depth records, a power of two, so a record's slot is its index masked)
+// and its counters in shared memory.  The indices are 32-bit: the stack empties
+// (both reset) long before they could wrap.
 struct WarpWork {
     uint32_t* stack;
-    unsigned long long sbot, stop;
+    uint32_t sbot, stop;
     unsigned long long* ct;
     __device__ __forceinline__ unsigned long long& cnt() const { return ct[CT_CNT]; }
     __device__ __forceinline__ unsigned long long& hsum() const { return ct[CT_HSUM]; }
@@ -808,15 +810,15 @@ __device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootVie
     const Bits<NW> rowM4 = bits_ldg<NW>(R.M4() + (uint64_t)v * W, W);
     {   // exclude child -> this warp's stack
         if (ww.stop - ww.sbot >= sp.stack_depth) { if (l == 0) raise_error(sp.ctr, KPLEX_ERR_INTERNAL); return false; }
-        uint32_t* dst = ww.stack + (ww.stop % sp.stack_depth) * SW;
+        uint32_t* dst = ww.stack + (ww.stop & (sp.stack_depth - 1)) * SW;
         Bits<NW> Cx = C, Xx = X;
         bits_clear(Cx, v);
         bits_set(Xx, v);
-        uint32_t* cdst = m.SC() + (uint32_t)(ww.stop % STACK_CACHE) * SW;   // shared-memory copy
+        uint32_t* cdst = m.SC() + (ww.stop % STACK_CACHE) * SW;   // shared-memory copy
         if (l == 0) {
             __stcg(dst + 0, t->root); __stcg(dst + 1, np | ((nc - 1) << 16)); __stcg(dst + 2, nx + 1); __stcg(dst + 3, 0u);
             cdst[0] = t->root; cdst[1] = np | ((nc - 1) << 16); cdst[2] = nx + 1; cdst[3] = 0u;
-            m.SCT()[ww.stop % STACK_CACHE] = (uint32_t)ww.stop;
+            m.SCT()[ww.stop % STACK_CACHE] = ww.stop;
         }
 #pragma unroll
         for (int j = 0; j < NW; ++j) {
@@ -1041,7 +1043,7 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
     bool tma_ok = true;
     if (l == 0) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"((unsigned)__cvta_generic_to_shared(&CT[15])) : "memory");
     __syncwarp();
-    WarpWork ww{sp.stacks + (uint64_t)warp * sp.stack_depth * SW, 0ull, 0ull, CT};
+    WarpWork ww{sp.stacks + (uint64_t)warp * sp.stack_depth * SW, 0u, 0u, CT};
     const unsigned long long resume_at = sp.pause_at / 2 > 0 ? sp.pause_at / 2 : 1;
     bool have = false, counted = false, ks_active = false, paused = false, is_idle = false;
     unsigned long long idle = 0;   // idle iterations counted toward spin_limit
@@ -1060,9 +1062,9 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
         // ---------------- local depth-first work
         if (!have && ww.stop > ww.sbot) {
             --ww.stop;
-            const uint32_t cs = (uint32_t)(ww.stop % STACK_CACHE);
-            if (m.SCT()[cs] == (uint32_t)ww.stop) load_record<NW>(m.SC() + cs * SW, Wt, &t, false);   // still cached
-            else load_record<NW>(ww.stack + (ww.stop % sp.stack_depth) * SW, Wt, &t, true);
+            const uint32_t cs = ww.stop % STACK_CACHE;
+            if (m.SCT()[cs] == ww.stop) load_record<NW>(m.SC() + cs * SW, Wt, &t, false);   // still cached
+            else load_record<NW>(ww.stack + (ww.stop & (sp.stack_depth - 1)) * SW, Wt, &t, true);
             have = true;
             __syncwarp();
         }
@@ -1082,7 +1084,7 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
                 }
                 give = __shfl_sync(FULL, give, 0);
                 if (give) {
-                    const uint32_t* src = ww.stack + (ww.sbot % sp.stack_depth) * SW;
+                    const uint32_t* src = ww.stack + (ww.sbot & (sp.stack_depth - 1)) * SW;
                     // the record becomes a unit of work before it can be seen (and taken)
                     if (l == 0) { atomicAdd(&sp.ctr->work, 1u); __threadfence(); }
                     __syncwarp();

@@ -63,7 +63,8 @@ __device__ __forceinline__ int row_and_popc(const uint32_t* __restrict__ row, co
 
 // ---------------------------------------------------------------- task pool
 // A ring is a control block (head, tail, cap) and one sequence word per slot in
-// device memory, plus the record data.  The data of the main pool is in HBM;
+// device memory, plus the record data.  cap is a power of two (a position's slot
+// is the position masked).  The data of the main pool is in HBM;
 // the spill ring keeps its data in mapped pinned host memory, so only plain
 // loads and stores cross the bus (no GPU atomics on host memory) and a
 // system-scope fence orders them before the sequence word is published.
@@ -96,7 +97,7 @@ static __device__ __forceinline__ bool ring_push(Ring r, uint32_t slot_words, un
         const unsigned long long cap = pool->cap;
         for (unsigned long long it = 0; it < spin_limit; ++it) {
             pos = atomicAdd(&pool->tail, 0ull);
-            const uint32_t seq = atomicAdd(&r.seq[pos % cap], 0u);
+            const uint32_t seq = atomicAdd(&r.seq[pos & (cap - 1)], 0u);
             const int dif = (int)(seq - (uint32_t)pos);
             if (dif == 0) {
                 if (atomicCAS(&pool->tail, pos, pos + 1) == pos) { ok = 1; break; }
@@ -113,7 +114,7 @@ static __device__ __forceinline__ bool ring_push(Ring r, uint32_t slot_words, un
         if (l == 0) stuck = atomicCAS(&ctr->stuck_once, 0u, 1u) == 0u;
         if (__shfl_sync(FULL, stuck, 0)) return true;
     }
-    const unsigned long long slot = pos % pool->cap;
+    const unsigned long long slot = pos & (pool->cap - 1);
     uint32_t* dst = r.data + slot * slot_words;
     for (unsigned i = l; i < slot_words; i += 32) __stcg(dst + i, rec_word(src, src_global, i));
     if (r.sys) __threadfence_system(); else __threadfence();
@@ -133,7 +134,7 @@ static __device__ __forceinline__ bool ring_pop(Ring r, uint32_t slot_words, uns
         const unsigned long long cap = pool->cap;
         for (unsigned long long it = 0; it < spin_limit; ++it) {
             pos = atomicAdd(&pool->head, 0ull);
-            const uint32_t seq = atomicAdd(&r.seq[pos % cap], 0u);
+            const uint32_t seq = atomicAdd(&r.seq[pos & (cap - 1)], 0u);
             const int dif = (int)(seq - (uint32_t)(pos + 1));
             if (dif == 0) {
                 if (atomicCAS(&pool->head, pos, pos + 1) == pos) { ok = 1; break; }
@@ -146,7 +147,7 @@ static __device__ __forceinline__ bool ring_pop(Ring r, uint32_t slot_words, uns
     if (!ok) return false;
     pos = __shfl_sync(FULL, pos, 0);
     const unsigned long long cap = pool->cap;
-    const unsigned long long slot = pos % cap;
+    const unsigned long long slot = pos & (cap - 1);
     __threadfence();
     const uint32_t* src = r.data + slot * slot_words;
     for (unsigned i = l; i < slot_words; i += 32) dst[i] = __ldcg(src + i);
