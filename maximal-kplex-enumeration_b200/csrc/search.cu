@@ -139,6 +139,29 @@ __device__ __forceinline__ int bits_list(const Bits<NW>& b, uint16_t* list) {
     for (int j = 0; j < NW; ++j) off += bits_to_list(b.w[j], list + off, 1024u * j);
     return off;
 }
+// the lists of two disjoint bitsets in one pass over their non-zero words: a's
+// members to la, b's to lb (both ascending)
+template <int NW>
+__device__ __forceinline__ void bits_list2(const Bits<NW>& a, const Bits<NW>& b, uint16_t* la, uint16_t* lb) {
+    const unsigned l = lane_id();
+    const unsigned below = (1u << l) - 1u;
+    int oa = 0, ob = 0;
+#pragma unroll
+    for (int j = 0; j < NW; ++j) {
+        unsigned nz = __ballot_sync(FULL, (a.w[j] | b.w[j]) != 0u);
+        while (nz) {
+            const int i = __ffs(nz) - 1;
+            nz &= nz - 1;
+            const unsigned wa = __shfl_sync(FULL, a.w[j], i), wb = __shfl_sync(FULL, b.w[j], i);
+            const uint16_t x = (uint16_t)(1024u * j + i * 32 + l);
+            if ((wa >> l) & 1u) la[oa + __popc(wa & below)] = x;
+            if ((wb >> l) & 1u) lb[ob + __popc(wb & below)] = x;
+            oa += __popc(wa);
+            ob += __popc(wb);
+        }
+    }
+    __syncwarp();
+}
 
 // ============================================================== k-search state (shared memory)
 // Layout in words, sized by the largest root n_max of the search:
@@ -717,8 +740,7 @@ __device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootVie
     bits_store(m.P(), P);
     bits_store(m.PC(), bits_or(P, C));
     __syncwarp();
-    bits_list(P, m.list());
-    bits_list(C, m.list() + np);
+    bits_list2(P, C, m.list(), m.list() + np);
     const int tot = (int)(np + nc);
     #pragma unroll 1
     for (int i = l; i < tot; i += 32) {
@@ -830,7 +852,6 @@ __device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootVie
         }
         __syncwarp();
         ++ww.stop;
-        if (l == 0) { ++ww.tasks(); ww.bb() += 12ull * W; }
     }
     // include child
     const uint32_t np1 = np + 1;
@@ -862,7 +883,6 @@ __device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootVie
         if (pc + k < (int)np1 + 1) continue;
         if (rowg_covers(A + c * W, m.SAT(), W)) atomicOr(&m.NC()[c >> 5], 1u << (c & 31));
     }
-    if (l == 0) ww.bb() += (unsigned long long)nc * 4ull * W;
     __syncwarp();
     const Bits<NW> C1 = bits_load<NW>(m.NC(), 32 * NW);
     const uint32_t nc1 = (uint32_t)bits_count(C1);
@@ -875,8 +895,11 @@ __device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootVie
         const uint32_t u = (i < (int)np) ? m.list()[i] : v;
         if (rowg_popc(A + u * W, m.PC(), W) + k < q) ub = false;
     }
-    if (l == 0) ww.bb() += (unsigned long long)np1 * 4ull * W;
-    if (!__all_sync(FULL, ub)) return false;
+    // rows read below: the exclude record (3), the C filter (nc), the upper bound (np + 1)
+    if (!__all_sync(FULL, ub)) {
+        if (l == 0) { ++ww.tasks(); ww.bb() += (unsigned long long)(nc + np1 + 3) * 4ull * W; }
+        return false;
+    }
     // X filter: class >= UNLINK2MORE and P' + x a k-plex
     const int nxl = bits_list(X, m.list());
     #pragma unroll 1
@@ -887,13 +910,13 @@ __device__ bool bnb_node(const SearchParams& sp, const BnbSmem& m, const RootVie
         const int px = rowg_popc_covers(A + x * W, m.P(), m.SAT(), W, &ok);
         if (ok && px + k >= (int)np1 + 1) atomicOr(&m.NX()[x >> 5], 1u << (x & 31));
     }
-    if (l == 0) ww.bb() += (unsigned long long)nxl * 4ull * W;
     __syncwarp();
     const Bits<NW> X1 = bits_load<NW>(m.NX(), 32 * NW);
     t->nx = (uint32_t)bits_count(X1);
     t->P = P1; t->C = C1; t->X = X1;
     t->np = np1; t->nc = nc1;
-    if (l == 0) { ++ww.tasks(); ww.bb() += 12ull * W; }
+    // and the X filter (nxl) and the include record (3)
+    if (l == 0) { ww.tasks() += 2; ww.bb() += (unsigned long long)(nc + np1 + nxl + 6) * 4ull * W; }
     return true;
 }
 
