@@ -90,13 +90,15 @@ struct Counters {
     unsigned int max_n, max_left, max_w, max_nw;
     unsigned int truncated, oversized, depth_capped;
     unsigned int error;            // KPLEX_ERR_* raised on the device (first one wins)
-    unsigned int next_root;        // k-search job dispenser
+    // the counters that many warps update during the search each start a line of
+    // their own, so that atomics on one do not queue behind atomics on another
+    alignas(128) unsigned int next_root;   // k-search job dispenser
     unsigned int ks_paused;        // k-search warps that stopped at the pause threshold
     unsigned int ks_active;        // k-search slots holding an unfinished root
-    unsigned int holders;          // warps holding work now (the idle-wait heuristic)
-    unsigned int work;             // outstanding work units: unclaimed k-search jobs, running jobs,
+    alignas(128) unsigned int holders;     // warps holding work now (the idle-wait heuristic)
+    alignas(128) unsigned int work;            // outstanding work units: unclaimed k-search jobs, running jobs,
                                    // records in the pool / block queues / spill ring, warps holding work
-    unsigned int bnb_done;         // branch warps that exited
+    alignas(128) unsigned int bnb_done;    // branch warps that exited
     unsigned int timeouts;         // bounded waits that gave up
     unsigned int decomp_next;      // decomposition root dispenser
     unsigned int pad[2];
@@ -113,10 +115,12 @@ struct Counters {
 
 // Vyukov bounded MPMC ring: each slot carries a sequence number so that a
 // producer and a consumer never touch the same record concurrently.
+// head, tail and the read-only capacity are on separate lines: takers hit the
+// head with atomics, givers the tail.
 struct Pool {
-    unsigned long long head;   // next slot to dequeue
-    unsigned long long tail;   // next slot to enqueue
-    unsigned long long cap;    // slots
+    alignas(128) unsigned long long head;   // next slot to dequeue
+    alignas(128) unsigned long long tail;   // next slot to enqueue
+    alignas(128) unsigned long long cap;    // slots
     unsigned long long pad;
 };
 

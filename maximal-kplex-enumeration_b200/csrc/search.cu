@@ -1299,7 +1299,7 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
             __threadfence();
             // one counter covers every place work can be (a unit moves, never
             // vanishes, when a record is taken), so zero means finished
-            done = atomicAdd(&sp.ctr->work, 0u) == 0u;
+            done = *(volatile unsigned*)&sp.ctr->work == 0u;   // a coherent load, not an atomic
             const unsigned live = *(volatile unsigned*)&sp.ctr->ks_active;
             others_busy = *(volatile unsigned*)&sp.ctr->holders > 0 || live > 0;
         }
