@@ -525,7 +525,7 @@ def main():
     ap.add_argument("--shard-mode", default="weighted", choices=["weighted", "modulo"],
                     help="multi-GPU root partition: cost-weighted (kplex_partition_roots) or r % world")
     ap.add_argument("--blocks-per-sm", type=int, default=0,
-                    help="plain: 8-warp blocks per SM of the search kernel (2 or 3; 0 = the library default)")
+                    help="plain: 9-warp blocks per SM of the search kernel (2 or 3; 0 = the library default)")
     ap.add_argument("--stage-after", type=int, default=0,
                     help="plain: branch nodes on one root before its adjacency matrix is staged in shared memory")
     ap.add_argument("--shards", type=int, default=1,

@@ -59,7 +59,7 @@ typedef struct {
     uint32_t omp_threads;   /* host threads for preprocessing (0 = all) */
     uint32_t shard_index;   /* multi-GPU root sharding: this call searches the roots whose */
     uint32_t shard_count;   /* degeneracy rank r has r % shard_count == shard_index (0/0 = all) */
-    uint32_t blocks_per_sm; /* persistent search kernel: 8-warp blocks per SM, 2 or 3 (0 = 2) */
+    uint32_t blocks_per_sm; /* persistent search kernel: 9-warp blocks per SM, 2 or 3 (0 = 2) */
     int32_t stage_after;    /* branch nodes a warp processes on one root before it copies the root's
                                adjacency matrix to shared memory (0 = 8, < 0 = never) */
     uint32_t root_begin;    /* search only the roots of degeneracy rank r in [root_begin, root_end) */

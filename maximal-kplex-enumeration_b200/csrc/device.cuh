@@ -45,6 +45,9 @@ constexpr int MAX_LEFT_WORDS = MAX_LEFT / 32;
 // local vertices) never fill and no root is abandoned here.
 constexpr int KS_MAX_DEPTH = MAX_LOCAL + 8;
 constexpr int MAX_K = 32;
+// warps per block of the persistent search kernel: one k-search producer and
+// SEARCH_WARPS - 1 branch-and-bound consumers
+constexpr int SEARCH_WARPS = 9;
 
 // root flags
 enum : uint32_t {

@@ -339,7 +339,7 @@ static int replay_capture(kplex_prepared* h, Replay& r, Workspace* d, bool per_g
     init_pool<<<d->sms * 4, 256, 0, st>>>(sp.pool_seq, r.cap, sp.pool);
     if (sp.spill_on) init_pool<<<d->sms * 4, 256, 0, st>>>(sp.spill_seq, r.scap, sp.spill_pool);
     cudaEventRecordWithFlags(r.ev[3], st, cudaEventRecordExternal);
-    if (h->nroots) kfn<<<r.blocks, 256, r.smem, st>>>(sp, r.nmax);
+    if (h->nroots) kfn<<<r.blocks, SEARCH_WARPS * 32, r.smem, st>>>(sp, r.nmax);
     cudaEventRecordWithFlags(r.ev[4], st, cudaEventRecordExternal);
     cudaMemcpyAsync(d->h_ctr, sp.ctr, sizeof(Counters), cudaMemcpyDeviceToHost, st);
     cudaMemcpyAsync(d->h_pool, sp.pool, sizeof(Pool), cudaMemcpyDeviceToHost, st);
@@ -386,7 +386,7 @@ static int replay_search(kplex_prepared* h, Replay& r, Workspace* d, kplex_resul
             x.status = (int)hc.error;
         }
     }
-    fill_result(h, hc, ms, t_dec, t_bnb, r.launches, r.blocks * 8, out);
+    fill_result(h, hc, ms, t_dec, t_bnb, r.launches, r.blocks * SEARCH_WARPS, out);
     return (int)hc.error;
 }
 
@@ -510,7 +510,7 @@ int search_impl(kplex_prepared* h, Workspace* d, kplex_result* out, kplex_result
     sp.pool_data = d->pool_data.as<uint32_t>();
     init_pool<<<d->sms * 4, 256, 0, st>>>(sp.pool_seq, cap, sp.pool);
     ++launches;
-    const int warps_per_block = 8;
+    const int warps_per_block = SEARCH_WARPS;
     // schedule knobs, from kplex_params only: blocks per SM the kernel is compiled for
     // (2 or 3) and how many nodes a warp processes on one root before copying its A to
     // shared memory
@@ -520,7 +520,7 @@ int search_impl(kplex_prepared* h, Workspace* d, kplex_result* out, kplex_result
     // one bitset word per lane while every root fits 1024 vertices, two beyond
     const uint32_t nw = search_words_per_lane(hc.max_w);
     const SearchKernel kfn = search_kernel_for(nw, minb);
-    // stage adjacency matrices in shared memory when minb 8-warp blocks still fit on an SM
+    // stage adjacency matrices in shared memory when minb blocks still fit on an SM
     int per_sm = 0;
     size_t smem_bytes = 0;
     for (int stage = sp.stage_after ? 1 : 0; stage >= 0; --stage) {

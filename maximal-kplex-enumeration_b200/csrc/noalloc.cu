@@ -185,7 +185,7 @@ extern "C" int kplex_search_noalloc(const uint32_t* d_off, const uint32_t* d_adj
     sp.Wt = Wt;
     sp.slot_words = 4 + 3 * Wt;
     size_t o2 = align_up(arena_off + (size_t)hc.arena_top * 4, 256);
-    const int warps_per_block = 8;
+    const int warps_per_block = SEARCH_WARPS;
     sp.a_words = 0;
     const uint32_t nw = search_words_per_lane(Wt);
     const SearchKernel kfn = search_kernel_for(nw, 3);

@@ -1339,10 +1339,12 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
 }
 
 // One body, compiled per bitset width (NW words per lane) and register budget:
-// MINB blocks of 256 threads per SM (2: up to 128 registers; 3: 80, with some
-// spills).  Roots above 1024 vertices need NW = 2, built for 2 blocks only.
+// MINB blocks of SEARCH_WARPS = 9 warps per SM (2: up to 112 registers, no
+// spills, 18 warps per SM; 3: 72, with spills).  Measured on soc-epinions:
+// 2 x 9 warps 510 ms, 2 x 8 533 ms, 2 x 10 (96 registers) 519 ms, 3 x 7 563 ms,
+// 3 x 6 572 ms.  Roots above 1024 vertices need NW = 2, built for 2 blocks only.
 template <int NW, int MINB>
-__global__ void __launch_bounds__(256, MINB) search_kernel(SearchParams sp, uint32_t nmax) { search_body<NW>(sp, nmax); }
+__global__ void __launch_bounds__(32 * SEARCH_WARPS, MINB) search_kernel(SearchParams sp, uint32_t nmax) { search_body<NW>(sp, nmax); }
 
 SearchKernel search_kernel_for(uint32_t nw, int minb) {
     if (nw > 1) return search_kernel<2, 2>;
