@@ -480,12 +480,15 @@ __device__ int ks_advance(const SearchParams& sp, const KsSlot<NW>& S, Emitted<N
 // ============================================================== branch-and-bound
 // Adjacency rows are read through a generic pointer: the warp's copy of the
 // root's A in shared memory when it fits, else the arena in global memory.
+// W is a multiple of 4 and at least 4: the first 16-byte chunk is outside the
+// loop (rows of up to 256 vertices take one or two chunks).
 __device__ __forceinline__ int rowg_popc(const uint32_t* row, const uint32_t* mask, unsigned W) {
-    int c = 0;
     const uint4* r4 = reinterpret_cast<const uint4*>(row);
     const uint4* m4 = reinterpret_cast<const uint4*>(mask);
+    const uint4 a0 = r4[0], m0 = m4[0];
+    int c = __popc(a0.x & m0.x) + __popc(a0.y & m0.y) + __popc(a0.z & m0.z) + __popc(a0.w & m0.w);
 #pragma unroll 1
-    for (unsigned w = 0; w < W / 4; ++w) {
+    for (unsigned w = 1; w < W / 4; ++w) {
         const uint4 a = r4[w], m = m4[w];
         c += __popc(a.x & m.x) + __popc(a.y & m.y) + __popc(a.z & m.z) + __popc(a.w & m.w);
     }
@@ -494,13 +497,14 @@ __device__ __forceinline__ int rowg_popc(const uint32_t* row, const uint32_t* ma
 // popcount of row & mask, and whether every bit of sat is in row
 __device__ __forceinline__ int rowg_popc_covers(const uint32_t* row, const uint32_t* mask, const uint32_t* sat,
                                                 unsigned W, bool* covers) {
-    int c = 0;
-    uint32_t miss = 0;
     const uint4* r4 = reinterpret_cast<const uint4*>(row);
     const uint4* m4 = reinterpret_cast<const uint4*>(mask);
     const uint4* s4 = reinterpret_cast<const uint4*>(sat);
+    const uint4 a0 = r4[0], m0 = m4[0], t0 = s4[0];
+    int c = __popc(a0.x & m0.x) + __popc(a0.y & m0.y) + __popc(a0.z & m0.z) + __popc(a0.w & m0.w);
+    uint32_t miss = (t0.x & ~a0.x) | (t0.y & ~a0.y) | (t0.z & ~a0.z) | (t0.w & ~a0.w);
 #pragma unroll 1
-    for (unsigned w = 0; w < W / 4; ++w) {
+    for (unsigned w = 1; w < W / 4; ++w) {
         const uint4 a = r4[w], m = m4[w], t = s4[w];
         c += __popc(a.x & m.x) + __popc(a.y & m.y) + __popc(a.z & m.z) + __popc(a.w & m.w);
         miss |= (t.x & ~a.x) | (t.y & ~a.y) | (t.z & ~a.z) | (t.w & ~a.w);
@@ -511,11 +515,12 @@ __device__ __forceinline__ int rowg_popc_covers(const uint32_t* row, const uint3
 
 // whether every bit of sat is in row
 __device__ __forceinline__ bool rowg_covers(const uint32_t* row, const uint32_t* sat, unsigned W) {
-    uint32_t miss = 0;
     const uint4* r4 = reinterpret_cast<const uint4*>(row);
     const uint4* s4 = reinterpret_cast<const uint4*>(sat);
+    const uint4 a0 = r4[0], t0 = s4[0];
+    uint32_t miss = (t0.x & ~a0.x) | (t0.y & ~a0.y) | (t0.z & ~a0.z) | (t0.w & ~a0.w);
 #pragma unroll 1
-    for (unsigned w = 0; w < W / 4; ++w) {
+    for (unsigned w = 1; w < W / 4; ++w) {
         const uint4 a = r4[w], t = s4[w];
         miss |= (t.x & ~a.x) | (t.y & ~a.y) | (t.z & ~a.z) | (t.w & ~a.w);
     }
@@ -525,12 +530,14 @@ __device__ __forceinline__ bool rowg_covers(const uint32_t* row, const uint32_t*
 // popcounts of row & m1 and row & m2 in one pass over the row
 __device__ __forceinline__ void rowg_popc2(const uint32_t* row, const uint32_t* m1, const uint32_t* m2, unsigned W,
                                            int& c1, int& c2) {
-    int a1 = 0, a2 = 0;
     const uint4* r4 = reinterpret_cast<const uint4*>(row);
     const uint4* x4 = reinterpret_cast<const uint4*>(m1);
     const uint4* y4 = reinterpret_cast<const uint4*>(m2);
+    const uint4 a0 = r4[0], x0 = x4[0], y0 = y4[0];
+    int a1 = __popc(a0.x & x0.x) + __popc(a0.y & x0.y) + __popc(a0.z & x0.z) + __popc(a0.w & x0.w);
+    int a2 = __popc(a0.x & y0.x) + __popc(a0.y & y0.y) + __popc(a0.z & y0.z) + __popc(a0.w & y0.w);
 #pragma unroll 1
-    for (unsigned w = 0; w < W / 4; ++w) {
+    for (unsigned w = 1; w < W / 4; ++w) {
         const uint4 a = r4[w], x = x4[w], y = y4[w];
         a1 += __popc(a.x & x.x) + __popc(a.y & x.y) + __popc(a.z & x.z) + __popc(a.w & x.w);
         a2 += __popc(a.x & y.x) + __popc(a.y & y.y) + __popc(a.z & y.z) + __popc(a.w & y.w);
