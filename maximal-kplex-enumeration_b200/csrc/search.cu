@@ -1203,9 +1203,21 @@ __device__ __forceinline__ void search_body(SearchParams sp, uint32_t nmax) {
                     }
                     j = __shfl_sync(FULL, j, 0);
                     if (j >= 0) {
-                        // root of job j: the last r with job_base[r] <= j
+                        // root of job j: the last r with job_base[r] <= j (job_base is
+                        // non-decreasing, job_base[0] = 0).  A 32-way search: each lane
+                        // probes one point of [lo2, hi2), the ballot of "<= j" is a prefix
+                        // of the lanes, and the interval shrinks 32-fold per round (four
+                        // dependent loads for a million roots instead of twenty).
                         uint32_t lo2 = 0, hi2 = sp.nroots;
-                        while (hi2 - lo2 > 1) { const uint32_t mid = (lo2 + hi2) >> 1; if (__ldg(sp.job_base + mid) <= (uint32_t)j) lo2 = mid; else hi2 = mid; }
+                        while (hi2 - lo2 > 1) {
+                            const uint32_t step = (hi2 - lo2 + 31u) >> 5;
+                            const uint32_t p = lo2 + (l + 1u) * step;
+                            const bool le = p < hi2 && __ldg(sp.job_base + p) <= (uint32_t)j;
+                            const uint32_t c = (uint32_t)__popc(__ballot_sync(FULL, le));
+                            const uint32_t nlo = lo2 + c * step;
+                            hi2 = min(nlo + step, hi2);
+                            lo2 = nlo;
+                        }
                         const RootDesc rd = sp.roots[lo2];
                         ks_start<NW>(sp, S, lo2, (uint32_t)j - __ldg(sp.job_base + lo2), rd);
                         ks_active = true;
